@@ -1,0 +1,334 @@
+"""B200 blob encoder for the 0G DA encoder path — Python host binding.
+
+Mirrors the reference's host interface over the C ABI of
+include/zg_encoder.h (ctypes):
+
+  reference (0glabs/0g-da-encoder)                   here
+  -------------------------------------------------  ---------------------------
+  constants BLOB_ROW_LOG/BLOB_COL_LOG/...             Dims
+  (crates/encoder/src/constants.rs:14-28)
+  RawData::try_from(&[u8]) (raw_data.rs:76-95)        RawData.try_from(bytes)
+  EncoderError::TooLargeBlob (encoder/error.rs:3-6)   TooLargeBlob
+  ZgEncoderParams::from_dir_mont (blob/encode.rs:114) ZgEncoderParams.from_dir_mont
+  PowerTau::setup_inner(Some(tau)) + from_pp          ZgEncoderParams.from_seed
+  EncodedBlob::build/get_row/get_commitment/...       EncodedBlob
+  (crates/encoder/src/encoder/blob.rs:32-62)
+  EncoderService::process_data (grpc/src/service.rs)  EncoderService.process_data
+  EncodeBlobReply (grpc/proto/encoder.proto:16-22)    EncodeBlobReply
+
+All compute runs in the CUDA library; there is no CPU fallback. Importing
+works without a GPU; creating params requires one.
+"""
+import ctypes
+import os
+from dataclasses import dataclass, field
+from typing import List
+
+from . import build as _build
+
+__all__ = [
+    "Dims", "RawData", "EncoderError", "TooLargeBlob", "ZgEncoderParams", "EncodedBlob",
+    "EncodeBlobReply", "EncoderService", "lib", "LIB_PATH", "C_ABI_FUNCTIONS",
+]
+
+LIB_PATH = _build.LIB
+_lib = None
+
+ZG_OK = 0
+ZG_ERR_TOO_LARGE_BLOB = 1
+
+
+class _Config(ctypes.Structure):
+    _fields_ = [
+        ("log_row", ctypes.c_uint32),
+        ("log_col", ctypes.c_uint32),
+        ("tau_seed", ctypes.c_uint64),
+        ("params_dir", ctypes.c_char_p),
+        ("device", ctypes.c_int),
+    ]
+
+
+class _DeviceBlob(ctypes.Structure):
+    _fields_ = [
+        ("encoded_data", ctypes.c_void_p),
+        ("slices", ctypes.c_void_p),
+        ("slice_size", ctypes.c_size_t),
+        ("amt_outputs", ctypes.c_void_p),
+        ("roots", ctypes.c_void_p),
+        ("file_root", ctypes.c_void_p),
+    ]
+
+
+_P = ctypes.c_void_p
+_SZ = ctypes.c_size_t
+_SIGS = {
+    "zg_ctx_create": (ctypes.c_int, [ctypes.POINTER(_Config), ctypes.POINTER(_P)]),
+    "zg_ctx_destroy": (None, [_P]),
+    "zg_ctx_warmup": (ctypes.c_int, [_P]),
+    "zg_encode": (ctypes.c_int, [_P, ctypes.c_char_p, _SZ, ctypes.c_int, ctypes.POINTER(_P)]),
+    "zg_reply_free": (None, [_P]),
+    "zg_reply_version": (ctypes.c_uint32, [_P]),
+    "zg_reply_erasure_commitment": (_P, [_P, ctypes.POINTER(_SZ)]),
+    "zg_reply_storage_root": (_P, [_P, ctypes.POINTER(_SZ)]),
+    "zg_reply_encoded_data": (_P, [_P, ctypes.POINTER(_SZ)]),
+    "zg_reply_num_slices": (_SZ, [_P]),
+    "zg_reply_slice": (_P, [_P, _SZ, ctypes.POINTER(_SZ)]),
+    "zg_reply_roots": (_P, [_P, ctypes.POINTER(_SZ)]),
+    "zg_encode_device": (ctypes.c_int, [_P, _P, _SZ, _P, ctypes.POINTER(_DeviceBlob)]),
+    "zg_ctx_param_line": (ctypes.c_int, [_P, ctypes.c_int, ctypes.c_int, _P, _SZ]),
+    "zg_msm_chunks": (ctypes.c_int, [_P, _P, ctypes.c_uint32, ctypes.c_uint32, ctypes.c_uint32, _P, _P]),
+    "zg_ntt": (ctypes.c_int, [_P, ctypes.c_uint32, ctypes.c_uint32, ctypes.c_int, ctypes.c_uint32, _P]),
+    "zg_merkle_roots": (ctypes.c_int, [_P, _SZ, _P, _P]),
+    "zg_selftest": (ctypes.c_int, [ctypes.POINTER(ctypes.c_int), ctypes.c_int]),
+    "zg_last_error": (ctypes.c_char_p, []),
+}
+C_ABI_FUNCTIONS = sorted(_SIGS)
+
+
+def lib(build_if_missing=True):
+    """The loaded CUDA library. Raises if it is missing and cannot be built."""
+    global _lib
+    if _lib is None:
+        if build_if_missing:
+            _build.build()
+        if not os.path.exists(LIB_PATH):
+            raise RuntimeError(f"CUDA encoder library missing: {LIB_PATH}")
+        L = ctypes.CDLL(LIB_PATH)
+        for name, (res, args) in _SIGS.items():
+            fn = getattr(L, name)
+            fn.restype = res
+            fn.argtypes = args
+        _lib = L
+    return _lib
+
+
+def _check(rc):
+    if rc == ZG_OK:
+        return
+    msg = lib().zg_last_error().decode(errors="replace")
+    if rc == ZG_ERR_TOO_LARGE_BLOB:
+        raise TooLargeBlob.from_message(msg)
+    raise RuntimeError(f"zg_encoder error {rc}: {msg}")
+
+
+@dataclass(frozen=True)
+class Dims:
+    """Blob geometry (crates/encoder/src/constants.rs:14-28)."""
+    log_row: int = 10
+    log_col: int = 10
+    coset_n: int = 3
+
+    @property
+    def rows(self):
+        return 1 << self.log_row
+
+    @property
+    def cols(self):
+        return 1 << self.log_col
+
+    @property
+    def raw_blob_size(self):
+        return self.rows * self.cols
+
+    @property
+    def rows_encoded(self):
+        return self.rows * self.coset_n
+
+    @property
+    def encoded_blob_size(self):
+        return self.rows_encoded * self.cols
+
+    @property
+    def max_blob_size(self):
+        return 31 * self.raw_blob_size
+
+    @property
+    def max_raw_data_size(self):
+        return self.max_blob_size - 4
+
+    @property
+    def slice_size(self):
+        return 312 + 32 * self.cols + 160 * self.log_row
+
+
+def selftest():
+    """Mismatch counts of the device arithmetic against its host build."""
+    fails = (ctypes.c_int * 7)()
+    _check(lib().zg_selftest(fails, 7))
+    return dict(zip(["fq_mul", "fq_mul_imm", "fq_add", "fq_sub", "fr_mul", "fr_roundtrip", "xyzz_dbl"],
+                    list(fails)))
+
+
+class EncoderError(Exception):
+    pass
+
+
+class TooLargeBlob(EncoderError):
+    """EncoderError::TooLargeBlob { actual, expected_max }."""
+
+    def __init__(self, actual, expected_max):
+        super().__init__(f"TooLargeBlob {{ actual: {actual}, expected_max: {expected_max} }}")
+        self.actual = actual
+        self.expected_max = expected_max
+
+    @classmethod
+    def from_message(cls, msg):
+        import re
+        m = re.search(r"actual: (\d+), expected_max: (\d+)", msg)
+        return cls(int(m.group(1)), int(m.group(2))) if m else cls(-1, -1)
+
+    def __eq__(self, o):
+        return isinstance(o, TooLargeBlob) and (self.actual, self.expected_max) == (o.actual, o.expected_max)
+
+
+class RawData:
+    """RawData: payload zero-padded to MAX_BLOB_SIZE with its LE u32 length in
+    the last four bytes (crates/encoder/src/raw_data.rs:8-95)."""
+
+    def __init__(self, padded: bytes, dims: Dims):
+        self.padded = padded
+        self.dims = dims
+
+    @classmethod
+    def try_from(cls, value: bytes, dims: Dims = Dims()):
+        n = len(value)
+        if n > dims.max_raw_data_size:
+            raise TooLargeBlob(n, dims.max_raw_data_size)
+        buf = bytearray(dims.max_blob_size)
+        buf[:n] = value
+        buf[dims.max_raw_data_size:] = n.to_bytes(4, "little")
+        return cls(bytes(buf), dims)
+
+    def as_bytes(self):
+        n = int.from_bytes(self.padded[self.dims.max_raw_data_size:], "little")
+        return self.padded[:n]
+
+
+class ZgEncoderParams:
+    """Device-resident encoder params of one GPU (a zg_ctx)."""
+
+    def __init__(self, handle, dims: Dims):
+        self._h = handle
+        self.dims = dims
+
+    @classmethod
+    def from_seed(cls, log_row=10, log_col=10, seed=0, device=0):
+        """Params of a seeded tau, built on the GPU by the reference builder's
+        rules (power_tau.rs:54-80, prove_params/generate.rs:139-263)."""
+        cfg = _Config(log_row, log_col, seed, None, device)
+        h = ctypes.c_void_p()
+        _check(lib().zg_ctx_create(ctypes.byref(cfg), ctypes.byref(h)))
+        return cls(h, Dims(log_row, log_col))
+
+    @classmethod
+    def from_dir_mont(cls, params_dir, log_row=10, log_col=10, device=0):
+        """Params from the reference's mont files (amt-prove-coset{c}-mont-*.bin)."""
+        cfg = _Config(log_row, log_col, 0, os.fsencode(params_dir), device)
+        h = ctypes.c_void_p()
+        _check(lib().zg_ctx_create(ctypes.byref(cfg), ctypes.byref(h)))
+        return cls(h, Dims(log_row, log_col))
+
+    @property
+    def handle(self):
+        return self._h
+
+    def warmup(self):
+        _check(lib().zg_ctx_warmup(self._h))
+
+    def param_line(self, coset, line):
+        n = self.dims.raw_blob_size * 64
+        buf = ctypes.create_string_buffer(n)
+        _check(lib().zg_ctx_param_line(self._h, coset, line, buf, n))
+        return buf.raw
+
+    def close(self):
+        if self._h:
+            lib().zg_ctx_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+@dataclass
+class EncodeBlobReply:
+    """grpc/proto/encoder.proto:16-22."""
+    version: int = 0
+    erasure_commitment: bytes = b""
+    storage_root: bytes = b""
+    encoded_data: bytes = b""
+    encoded_slice: List[bytes] = field(default_factory=list)
+
+
+def _encode_raw(params: ZgEncoderParams, data: bytes, require_data: bool):
+    L = lib()
+    r = ctypes.c_void_p()
+    _check(L.zg_encode(params.handle, data, len(data), 1 if require_data else 0, ctypes.byref(r)))
+    try:
+        n = ctypes.c_size_t()
+
+        def grab(ptr):
+            return ctypes.string_at(ptr, n.value) if n.value else b""
+
+        com = grab(L.zg_reply_erasure_commitment(r, ctypes.byref(n)))
+        root = grab(L.zg_reply_storage_root(r, ctypes.byref(n)))
+        edata = grab(L.zg_reply_encoded_data(r, ctypes.byref(n)))
+        roots = grab(L.zg_reply_roots(r, ctypes.byref(n)))
+        ns = L.zg_reply_num_slices(r)
+        first = L.zg_reply_slice(r, 0, ctypes.byref(n))
+        size = n.value
+        blob = ctypes.string_at(first, size * ns)
+        slices = [blob[i * size:(i + 1) * size] for i in range(ns)]
+        return L.zg_reply_version(r), com, root, edata, roots, slices
+    finally:
+        L.zg_reply_free(r)
+
+
+class EncodedBlob:
+    """EncodedBlob (crates/encoder/src/encoder/blob.rs:26-62), host copy of the
+    device results; slices are the ark-serialized EncodedSlice bytes."""
+
+    def __init__(self, commitment, roots, file_root, data, slices):
+        self._commitment = commitment
+        self._roots = roots
+        self._file_root = file_root
+        self._data = data
+        self._slices = slices
+
+    @classmethod
+    def build(cls, raw: bytes, params: ZgEncoderParams):
+        """EncodedBlob::build over RawData::try_from(raw) (raises TooLargeBlob)."""
+        _, com, root, edata, roots, slices = _encode_raw(params, raw, True)
+        return cls(com, roots, root, edata, slices)
+
+    def get_row(self, index) -> bytes:
+        assert index < len(self._slices)
+        return self._slices[index]
+
+    def get_affine_commitment(self) -> bytes:
+        return self._commitment
+
+    get_commitment = get_affine_commitment
+
+    def get_roots(self):
+        return [self._roots[32 * i:32 * (i + 1)] for i in range(3)]
+
+    def get_file_root(self) -> bytes:
+        return self._file_root
+
+    def get_data(self) -> bytes:
+        return self._data
+
+
+class EncoderService:
+    """EncoderService (grpc/src/service.rs:30-105) over device params."""
+
+    def __init__(self, params: ZgEncoderParams):
+        self.params = params
+
+    def process_data(self, data: bytes, require_data: bool) -> EncodeBlobReply:
+        version, com, root, edata, _, slices = _encode_raw(self.params, data, require_data)
+        return EncodeBlobReply(version, com, root, edata, slices)

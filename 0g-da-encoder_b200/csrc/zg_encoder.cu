@@ -1,0 +1,841 @@
+// Host orchestration and C ABI of the B200 blob encoder (include/zg_encoder.h).
+//
+// One zg_ctx owns one device's params (3 cosets x (LR+2) G1 lines, resident
+// in HBM for the context's lifetime, the role of AMTParams' lazily uploaded
+// MsmBasisOnDevice in crates/amt/src/prove_params/prove_gpu.rs:30-53), the
+// twiddle tables and the per-blob scratch. Encodes on one context are
+// serialised by a mutex; use one context per stream of work for overlap.
+#include <cuda_runtime.h>
+#include <dirent.h>
+
+#include <cstdio>
+#include <cstring>
+#include <map>
+#include <mutex>
+#include <string>
+#include <vector>
+
+#include "../../include/zg_encoder.h"
+#include "zg_kernels.cuh"
+
+using namespace zg;
+
+namespace {
+
+thread_local std::string g_err;
+int fail(int code, const std::string& m) {
+  g_err = m;
+  return code;
+}
+#define ZG_CK(x)                                                                         \
+  do {                                                                                   \
+    cudaError_t e_ = (x);                                                                \
+    if (e_ != cudaSuccess) return fail(ZG_ERR_CUDA, std::string(#x) + ": " + cudaGetErrorString(e_)); \
+  } while (0)
+
+uint32_t host_brev(uint32_t x, int bits) {
+  uint32_t r = 0;
+  for (int i = 0; i < bits; ++i) r = (r << 1) | ((x >> i) & 1);
+  return r;
+}
+
+// Fr two-adic root of unity 5^((r-1)/2^28) (ark-bn254 FrConfig generator 5)
+Fr fr_two_adic_root() {
+  Fr c;
+  const uint32_t w[8] = {0x725b19f0u, 0x9bd61b6eu, 0x41112ed4u, 0x402d111eu,
+                         0x8ef62abcu, 0x00e0a7ebu, 0xa58a7e85u, 0x2a3c09f0u};
+  for (int i = 0; i < 8; ++i) c.v[i] = w[i];
+  return Fr::from_canonical(c);
+}
+Fr fr_root(int log_n) {
+  Fr w = fr_two_adic_root();
+  for (int i = log_n; i < 28; ++i) w = w.sqr();
+  return w;
+}
+// AMTParams::coset_factor (crates/amt/src/prove_params/generate.rs:128-137)
+Fr coset_factor(int log_len, uint32_t idx) {
+  uint32_t pow = host_brev(idx, 28 - log_len);
+  return fr_two_adic_root().pow_u64(pow);
+}
+
+uint64_t splitmix64(uint64_t& s) {
+  uint64_t z = (s += 0x9e3779b97f4a7c15ULL);
+  z = (z ^ (z >> 30)) * 0xbf58476d1ce4e5b9ULL;
+  z = (z ^ (z >> 27)) * 0x94d049bb133111ebULL;
+  return z ^ (z >> 31);
+}
+// tau = (w0 + w1 2^64 + ... + w7 2^448) mod r, w_i the SplitMix64 stream at `seed`
+Fr tau_from_seed(uint64_t seed) {
+  uint64_t s = seed, w[8];
+  for (int i = 0; i < 8; ++i) w[i] = splitmix64(s);
+  auto reduce = [](const uint64_t* x) {
+    Fr a;
+    for (int i = 0; i < 4; ++i) {
+      a.v[2 * i] = (uint32_t)x[i];
+      a.v[2 * i + 1] = (uint32_t)(x[i] >> 32);
+    }
+    for (;;) {
+      Fr d;
+      if (Fr::sub_raw(d, a, Fr::modulus())) break;
+      a = d;
+    }
+    return Fr::from_canonical(a);
+  };
+  Fr lo = reduce(w), hi = reduce(w + 4);
+  Fr two256 = Fr::from_canonical(Fr::one());  // 2^256 mod r as a field element
+  return lo + hi * two256;
+}
+
+Fr host_fr_from_u32(uint32_t x) { return Fr::from_u32(x); }
+
+// twiddle tables for an N = R * C transform
+struct Twiddles {
+  int lr = 0, lc = 0;
+  Fr *twf_c = nullptr, *twi_c = nullptr, *twf_r = nullptr, *twi_r = nullptr;
+  Fr *wn_lo = nullptr, *wn_hi = nullptr, *wni_lo = nullptr, *wni_hi = nullptr;
+  Fr *gs_lo = nullptr, *gs_hi = nullptr;  // coset scale tables (cosets 1, 2)
+};
+
+template <class T>
+int upload(T** dst, const std::vector<T>& v) {
+  ZG_CK(cudaMalloc(dst, sizeof(T) * std::max<size_t>(v.size(), 1)));
+  ZG_CK(cudaMemcpy(*dst, v.data(), sizeof(T) * v.size(), cudaMemcpyHostToDevice));
+  return 0;
+}
+std::vector<Fr> pow_table(const Fr& x, size_t n) {
+  std::vector<Fr> t(n);
+  Fr a = Fr::one();
+  for (size_t i = 0; i < n; ++i) { t[i] = a; a = a * x; }
+  return t;
+}
+int make_twiddles(int lr, int lc, Twiddles* tw) {
+  tw->lr = lr;
+  tw->lc = lc;
+  const size_t R = size_t(1) << lr, C = size_t(1) << lc, N = R * C;
+  Fr wc = fr_root(lc), wr = fr_root(lr), wn = fr_root(lr + lc);
+  int rc = 0;
+  if ((rc = upload(&tw->twf_c, pow_table(wc, std::max<size_t>(C / 2, 1))))) return rc;
+  if ((rc = upload(&tw->twi_c, pow_table(wc.inverse(), std::max<size_t>(C / 2, 1))))) return rc;
+  if ((rc = upload(&tw->twf_r, pow_table(wr, std::max<size_t>(R / 2, 1))))) return rc;
+  if ((rc = upload(&tw->twi_r, pow_table(wr.inverse(), std::max<size_t>(R / 2, 1))))) return rc;
+  if ((rc = upload(&tw->wn_lo, pow_table(wn, C)))) return rc;
+  if ((rc = upload(&tw->wn_hi, pow_table(wn.pow_u64(C), R)))) return rc;
+  Fr wni = wn.inverse();
+  if ((rc = upload(&tw->wni_lo, pow_table(wni, C)))) return rc;
+  if ((rc = upload(&tw->wni_hi, pow_table(wni.pow_u64(C), R)))) return rc;
+  Fr ninv = host_fr_from_u32((uint32_t)N).inverse();
+  std::vector<Fr> lo, hi;
+  for (int c = 1; c <= 2; ++c) {
+    Fr g = coset_factor(lr + lc, c);
+    std::vector<Fr> a = pow_table(g, C);
+    for (auto& x : a) x = x * ninv;
+    lo.insert(lo.end(), a.begin(), a.end());
+    std::vector<Fr> b = pow_table(g.pow_u64(C), R);
+    hi.insert(hi.end(), b.begin(), b.end());
+  }
+  if ((rc = upload(&tw->gs_lo, lo))) return rc;
+  if ((rc = upload(&tw->gs_hi, hi))) return rc;
+  return 0;
+}
+void free_twiddles(Twiddles* tw) {
+  Fr* ps[] = {tw->twf_c, tw->twi_c, tw->twf_r, tw->twi_r, tw->wn_lo, tw->wn_hi,
+              tw->wni_lo, tw->wni_hi, tw->gs_lo, tw->gs_hi};
+  for (Fr* p : ps) if (p) cudaFree(p);
+  *tw = Twiddles();
+}
+
+size_t msm_smem_bytes(int lc) {
+  size_t C = size_t(1) << lc;
+  return C * 32 + (size_t)MSM_WINDOWS * C * 2 + MSM_WINDOWS * 129 * 2 + 129 * 4 + 16;
+}
+
+int set_smem_limits() {
+  static bool done = false;
+  static std::mutex m;
+  std::lock_guard<std::mutex> g(m);
+  if (done) return 0;
+  const int big = 227 * 1024;
+  ZG_CK(cudaFuncSetAttribute(k_rows_from_raw, cudaFuncAttributeMaxDynamicSharedMemorySize, big));
+  ZG_CK(cudaFuncSetAttribute(k_cols, cudaFuncAttributeMaxDynamicSharedMemorySize, big));
+  ZG_CK(cudaFuncSetAttribute(k_rows_ntt, cudaFuncAttributeMaxDynamicSharedMemorySize, big));
+  ZG_CK(cudaFuncSetAttribute(k_msm_chunks, cudaFuncAttributeMaxDynamicSharedMemorySize, big));
+  ZG_CK(cudaFuncSetAttribute(k_ntt4_colpass, cudaFuncAttributeMaxDynamicSharedMemorySize, big));
+  ZG_CK(cudaFuncSetAttribute(k_ntt4_rowpass, cudaFuncAttributeMaxDynamicSharedMemorySize, big));
+  done = true;
+  return 0;
+}
+
+inline unsigned nblk(size_t n, unsigned t) { return (unsigned)((n + t - 1) / t); }
+
+// natural-order N-point transform out = DFT(x) (or inverse without 1/N), via
+// the column / row passes; tmp has N elements
+void ntt4(const Twiddles& tw, const Fr* x, Fr* tmp, Fr* out, bool inverse, cudaStream_t s) {
+  const int lr = tw.lr, lc = tw.lc;
+  const size_t R = size_t(1) << lr, C = size_t(1) << lc;
+  k_ntt4_colpass<<<(unsigned)C, 256, R * sizeof(Fr), s>>>(x, tmp, lr, lc, inverse ? tw.twi_r : tw.twf_r,
+                                                          inverse ? tw.wni_lo : tw.wn_lo,
+                                                          inverse ? tw.wni_hi : tw.wn_hi);
+  k_ntt4_rowpass<<<(unsigned)R, 256, C * sizeof(Fr), s>>>(tmp, out, lr, lc, inverse ? tw.twi_c : tw.twf_c);
+}
+
+}  // namespace
+
+struct zg_ctx {
+  int device = 0;
+  int lr = 0, lc = 0, L = 0;
+  size_t R = 0, C = 0, N = 0;
+  size_t max_blob = 0, max_raw = 0;
+  cudaStream_t stream = nullptr;
+  Twiddles tw;
+  G1Aff* bases = nullptr;  // [3][L][N]
+  uint8_t* raw = nullptr;
+  uint8_t* enc = nullptr;
+  Fr* T1 = nullptr;
+  Fr* Bc = nullptr;
+  XYZZ* win = nullptr;
+  XYZZ* part = nullptr;
+  XYZZ* nodes = nullptr;
+  uint8_t* amt = nullptr;
+  uint8_t* tree = nullptr;
+  uint64_t* tree_off_d = nullptr;
+  std::vector<uint64_t> tree_off;
+  int tree_depth = 0;  // leaves live at level tree_depth
+  size_t tree_bytes = 0;
+  uint8_t* slices = nullptr;
+  size_t slice_size = 0;
+  uint8_t* file_root = nullptr;
+  uint8_t* h_in = nullptr;  // pinned staging for payloads
+  std::mutex mu;
+};
+
+struct zg_reply {
+  uint32_t version = 0;
+  uint8_t commitment[64];
+  uint8_t storage_root[32];
+  uint8_t roots[96];
+  uint8_t* data = nullptr;  // pinned
+  size_t data_len = 0;
+  uint8_t* slices = nullptr;  // pinned
+  size_t slice_size = 0, nslices = 0;
+};
+
+namespace {
+
+int alloc_blob_buffers(zg_ctx* c) {
+  const size_t N = c->N, R = c->R;
+  ZG_CK(cudaMalloc(&c->raw, c->max_blob + 16));
+  ZG_CK(cudaMalloc(&c->enc, 3 * N * 32));
+  ZG_CK(cudaMalloc(&c->T1, N * sizeof(Fr)));
+  ZG_CK(cudaMalloc(&c->Bc, 2 * N * sizeof(Fr)));
+  ZG_CK(cudaMalloc(&c->win, 3 * (size_t)c->L * R * MSM_WINDOWS * sizeof(XYZZ)));
+  ZG_CK(cudaMalloc(&c->part, 3 * (size_t)c->L * R * sizeof(XYZZ)));
+  ZG_CK(cudaMalloc(&c->nodes, 3 * (4 * R - 2) * sizeof(XYZZ)));
+  ZG_CK(cudaMalloc(&c->amt, 3 * (4 * R - 2) * 64));
+  // Merkle levels: level d holds 3 * 2^d nodes; leaves at depth LR + LC - 3
+  c->tree_depth = c->lr + c->lc - 3;
+  c->tree_off.assign(c->tree_depth + 1, 0);
+  size_t off = 0;
+  for (int d = 0; d <= c->tree_depth; ++d) {
+    c->tree_off[d] = off;
+    off += (size_t)3 * ((size_t)1 << d) * 32;
+  }
+  c->tree_bytes = off;
+  ZG_CK(cudaMalloc(&c->tree, off));
+  ZG_CK(cudaMalloc(&c->tree_off_d, c->tree_off.size() * sizeof(uint64_t)));
+  ZG_CK(cudaMemcpy(c->tree_off_d, c->tree_off.data(), c->tree_off.size() * sizeof(uint64_t), cudaMemcpyHostToDevice));
+  c->slice_size = 312 + 32 * c->C + 160 * (size_t)c->lr;
+  ZG_CK(cudaMalloc(&c->slices, 3 * R * c->slice_size));
+  ZG_CK(cudaMalloc(&c->file_root, 32));
+  ZG_CK(cudaMallocHost(&c->h_in, c->max_blob + 16));
+  return 0;
+}
+
+// Seeded params on the device: with tau known every param point is s * G1 for
+// a scalar s given by the Fr versions of the EC FFT formulas of
+// AMTParams::from_pp (generate.rs:139-232):
+//   basis      = enact(ifft(tau'^i))
+//   quotient_d = enact(fft(c_d) / N),  c_d[i] = tau'^(M-i) for 1 <= i <= M = N >> d
+//   high_basis = enact(tau^(3N) * ifft(tau'^i))
+// with tau' = tau / coset_factor(N, c) (generate.rs:152-170) and enact =
+// normalize + index_reverse (generate.rs:122-126).
+int build_seeded_params(zg_ctx* c, uint64_t seed) {
+  const size_t N = c->N;
+  const int ln = c->lr + c->lc;
+  cudaStream_t s = c->stream;
+  Fr tau = tau_from_seed(seed);
+  Fr* pw = nullptr;
+  Fr* sc = nullptr;
+  Fr* tmp = nullptr;
+  Fr* coeff = nullptr;
+  XYZZ* tabx = nullptr;
+  G1Aff* tab = nullptr;
+  ZG_CK(cudaMalloc(&pw, N * sizeof(Fr)));
+  ZG_CK(cudaMalloc(&sc, N * sizeof(Fr)));
+  ZG_CK(cudaMalloc(&tmp, N * sizeof(Fr)));
+  ZG_CK(cudaMalloc(&coeff, N * sizeof(Fr)));
+  ZG_CK(cudaMalloc(&tabx, 32 * 255 * sizeof(XYZZ)));
+  ZG_CK(cudaMalloc(&tab, 32 * 255 * sizeof(G1Aff)));
+  G1Aff g;
+  g.x = Fq::from_u32(1);
+  g.y = Fq::from_u32(2);
+  k_fixed_table<<<1, 32, 0, s>>>(tabx, g);
+  k_xyzz_to_affine<<<nblk(32 * 255, 256), 256, 0, s>>>(tabx, tab, 32 * 255);
+  Fr ninv = host_fr_from_u32((uint32_t)N).inverse();
+  Fr tau_hs = tau.pow_u64((uint64_t)3 * N);  // high_start = 2^(depth+2) - 2^depth
+  const unsigned T = 256;
+  for (int cs = 0; cs < 3; ++cs) {
+    Fr tp = cs ? tau * coset_factor(ln, cs).inverse() : tau;
+    k_powers<<<nblk(N, T), T, 0, s>>>(tp, pw, (uint32_t)N);
+    G1Aff* lines = c->bases + (size_t)cs * c->L * N;
+    ntt4(c->tw, pw, tmp, sc, true, s);
+    k_scale<<<nblk(N, T), T, 0, s>>>(sc, ninv, (uint32_t)N);
+    k_fixed_mul<<<nblk(N, T), T, 0, s>>>(tab, sc, lines + (size_t)c->lr * N, (uint32_t)N, ln);
+    k_scale<<<nblk(N, T), T, 0, s>>>(sc, tau_hs, (uint32_t)N);
+    k_fixed_mul<<<nblk(N, T), T, 0, s>>>(tab, sc, lines + (size_t)(c->lr + 1) * N, (uint32_t)N, ln);
+    for (int d = 1; d <= c->lr; ++d) {
+      k_quot_coeff<<<nblk(N, T), T, 0, s>>>(pw, coeff, (uint32_t)(N >> d), (uint32_t)N);
+      ntt4(c->tw, coeff, tmp, sc, false, s);
+      k_scale<<<nblk(N, T), T, 0, s>>>(sc, ninv, (uint32_t)N);
+      k_fixed_mul<<<nblk(N, T), T, 0, s>>>(tab, sc, lines + (size_t)(d - 1) * N, (uint32_t)N, ln);
+    }
+  }
+  ZG_CK(cudaStreamSynchronize(s));
+  ZG_CK(cudaGetLastError());
+  cudaFree(pw); cudaFree(sc); cudaFree(tmp); cudaFree(coeff); cudaFree(tabx); cudaFree(tab);
+  return 0;
+}
+
+// reference mont files: amt-prove-coset{c}-mont-{hash}-{LR:02}-{LN:02}.bin
+// (crates/amt/src/utils.rs:20-45; format fast_serde_bn254.rs:20-88)
+int load_mont_params(zg_ctx* c, const char* dir) {
+  const int ln = c->lr + c->lc;
+  std::vector<uint8_t> hostline(c->N * 64);
+  for (int cs = 0; cs < 3; ++cs) {
+    char prefix[64], suffix[32];
+    snprintf(prefix, sizeof(prefix), "amt-prove-coset%d-mont-", cs);
+    snprintf(suffix, sizeof(suffix), "-%02d-%02d.bin", c->lr, ln);
+    std::string found;
+    DIR* dp = opendir(dir);
+    if (!dp) return fail(ZG_ERR_PARAMS, std::string("cannot open params dir ") + dir);
+    while (dirent* e = readdir(dp)) {
+      std::string n = e->d_name;
+      if (n.rfind(prefix, 0) == 0 && n.size() > strlen(suffix) &&
+          n.compare(n.size() - strlen(suffix), strlen(suffix), suffix) == 0) {
+        found = std::string(dir) + "/" + n;
+        break;
+      }
+    }
+    closedir(dp);
+    if (found.empty()) return fail(ZG_ERR_PARAMS, std::string("no ") + prefix + "*" + suffix + " in " + dir);
+    FILE* f = fopen(found.c_str(), "rb");
+    if (!f) return fail(ZG_ERR_PARAMS, "cannot open " + found);
+    uint8_t hdr[6];
+    bool ok = fread(hdr, 1, 6, f) == 6 && memcmp(hdr, "bamt", 4) == 0 && hdr[4] == ln && hdr[5] == c->lr;
+    ok = ok && fseek(f, 256, SEEK_CUR) == 0;  // g2, high_g2 (uncompressed G2, 128 B each)
+    G1Aff* lines = c->bases + (size_t)cs * c->L * c->N;
+    auto read_line = [&](G1Aff* dst) {
+      if (fread(hostline.data(), 1, hostline.size(), f) != hostline.size()) return false;
+      return cudaMemcpy(dst, hostline.data(), hostline.size(), cudaMemcpyHostToDevice) == cudaSuccess;
+    };
+    ok = ok && read_line(lines + (size_t)c->lr * c->N);  // basis
+    for (int d = 0; ok && d < c->lr; ++d) ok = read_line(lines + (size_t)d * c->N);
+    size_t van = 0;
+    for (int d = 0; d < c->lr; ++d) van += (size_t)128 << (d + 1);
+    ok = ok && fseek(f, (long)van, SEEK_CUR) == 0;
+    ok = ok && read_line(lines + (size_t)(c->lr + 1) * c->N);  // high_basis
+    fclose(f);
+    if (!ok) return fail(ZG_ERR_PARAMS, "malformed params file " + found);
+  }
+  return 0;
+}
+
+int check_launch() {
+  cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess) return fail(ZG_ERR_CUDA, std::string("kernel launch: ") + cudaGetErrorString(e));
+  return 0;
+}
+
+int merkle_levels(const uint8_t* items, size_t n_items, uint8_t* tree, const std::vector<uint64_t>& off,
+                  int depth, cudaStream_t s) {
+  const unsigned T = 128;
+  size_t leaves = n_items / 8;
+  k_merkle_leaves<<<nblk(leaves, T), T, 0, s>>>(items, tree + off[depth], (uint32_t)leaves);
+  for (int d = depth - 1; d >= 0; --d) {
+    size_t cnt = (size_t)3 << d;
+    k_merkle_parents<<<nblk(cnt, T), T, 0, s>>>(tree + off[d + 1], tree + off[d], (uint32_t)cnt);
+  }
+  return check_launch();
+}
+
+// the full per-blob pipeline on device; d_data holds `len` payload bytes
+int encode_device_locked(zg_ctx* c, const uint8_t* d_data, size_t len, cudaStream_t s) {
+  const int lr = c->lr, lc = c->lc;
+  const size_t R = c->R, C = c->C, N = c->N;
+  // RS extension: rows iNTT, column passes, rows NTT
+  k_rows_from_raw<<<(unsigned)R, 256, C * sizeof(Fr) + 31 * C, s>>>(
+      d_data, len, c->max_raw, lr, lc, c->enc, c->T1, c->tw.twi_c, c->tw.wni_lo, c->tw.wni_hi);
+  k_cols<<<nblk(C, COLS_PER_BLOCK), 256, 2 * R * sizeof(Fr), s>>>(c->T1, c->Bc, lr, lc, c->tw.twi_r, c->tw.twf_r,
+                                                                   c->tw.gs_lo, c->tw.gs_hi, c->tw.wn_lo,
+                                                                   c->tw.wn_hi);
+  k_rows_ntt<<<dim3((unsigned)R, 2), 256, C * sizeof(Fr), s>>>(c->Bc, c->enc, lr, lc, c->tw.twf_c);
+  int rc = check_launch();
+  if (rc) return rc;
+  // Merkle tree over the encoded data and the file root
+  if ((rc = merkle_levels(c->enc, 3 * N, c->tree, c->tree_off, c->tree_depth, s))) return rc;
+  k_file_root<<<1, 32, 0, s>>>(c->tree + c->tree_off[0], c->file_root);
+  // AMT: per-chunk MSMs, window combination, trees, serialisation
+  MsmChunkArgs a;
+  a.scalars = c->enc;
+  a.bases = c->bases;
+  a.win = c->win;
+  a.lr = lr;
+  a.lc = lc;
+  a.lines = c->L;
+  a.bitrev_rows = 1;
+  a.scalar_coset_stride = N;
+  a.base_coset_stride = (uint64_t)c->L * N;
+  k_msm_chunks<<<dim3((unsigned)R, 3), MSM_THREADS, msm_smem_bytes(lc), s>>>(a);
+  const uint32_t nmsm = (uint32_t)(3 * c->L * R);
+  k_msm_combine<<<nblk(nmsm, 64), 64, 0, s>>>(c->win, c->part, nmsm);
+  k_amt_tree<<<dim3((unsigned)c->L, 3), 512, 0, s>>>(c->part, c->nodes, lr, c->L);
+  const uint32_t nn = (uint32_t)(3 * (4 * R - 2));
+  k_serialize_nodes<<<nblk(nn, 128), 128, 0, s>>>(c->nodes, c->amt, nn);
+  SliceArgs sa;
+  sa.enc = c->enc;
+  sa.amt = c->amt;
+  sa.tree = c->tree;
+  sa.tree_off = c->tree_off_d;
+  sa.out = c->slices;
+  sa.lr = lr;
+  sa.lc = lc;
+  sa.slice_size = c->slice_size;
+  k_slices<<<(unsigned)(3 * R), 256, 0, s>>>(sa);
+  return check_launch();
+}
+
+std::mutex g_ntt_mu;
+std::map<std::pair<int, int>, Twiddles> g_ntt_tw;
+
+const Twiddles* cached_twiddles(int lr, int lc) {
+  std::lock_guard<std::mutex> g(g_ntt_mu);
+  auto key = std::make_pair(lr, lc);
+  auto it = g_ntt_tw.find(key);
+  if (it != g_ntt_tw.end()) return &it->second;
+  Twiddles t;
+  if (make_twiddles(lr, lc, &t)) return nullptr;
+  return &(g_ntt_tw[key] = t);
+}
+
+__global__ void k_canon_to_mont(Fr* v, uint64_t total, int logn, Fr g, int coset) {
+  uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= total) return;
+  Fr x = Fr::from_canonical(v[i]);
+  if (coset) x = x * g.pow_u64(i & ((1ull << logn) - 1));
+  v[i] = x;
+}
+__global__ void k_mont_to_canon(Fr* v, uint64_t n, Fr scale, int do_scale) {
+  uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  Fr x = v[i];
+  if (do_scale) x = x * scale;
+  v[i] = x.to_canonical();
+}
+// single-CTA transform of each contiguous vector (n <= 2048)
+__global__ void k_ntt_small(Fr* v, int logn, const Fr* tw) {
+  extern __shared__ __align__(16) uint8_t smem[];
+  Fr* s = reinterpret_cast<Fr*>(smem);
+  const int n = 1 << logn;
+  Fr* p = v + (size_t)blockIdx.x * n;
+  for (int i = threadIdx.x; i < n; i += blockDim.x) s[brev_bits(i, logn)] = p[i];
+  __syncthreads();
+  ntt_smem(s, logn, tw);
+  for (int i = threadIdx.x; i < n; i += blockDim.x) p[i] = s[i];
+}
+
+
+// device-vs-host arithmetic self test: out[k] counts mismatches of op k over
+// n input pairs (0 Fq mul, 1 Fq mul with immediate modulus, 2 Fq add, 3 Fq sub,
+// 4 Fr mul, 5 Fr canonical round trip, 6 XYZZ add vs doubling)
+__global__ void k_selftest(const Fq* a, const Fq* b, Fq* res, uint32_t n) {
+  uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  Fq x = a[i], y = b[i];
+  res[7 * i + 0] = Fq::mul(x, y);
+  res[7 * i + 1] = Fq::mul_imm(x, y);
+  res[7 * i + 2] = Fq::add(x, y);
+  res[7 * i + 3] = Fq::sub(x, y);
+  Fr xr = *reinterpret_cast<const Fr*>(&x), yr = *reinterpret_cast<const Fr*>(&y);
+  Fr m = Fr::mul(xr, yr);
+  res[7 * i + 4] = *reinterpret_cast<Fq*>(&m);
+  Fr rt = Fr::from_canonical(xr).to_canonical();
+  res[7 * i + 5] = *reinterpret_cast<Fq*>(&rt);
+  // P + P via add() must equal dbl(); P = (x, y) is not on the curve, the
+  // formulas are still polynomial identities in the coordinates
+  XYZZ p1 = XYZZ::from_affine(G1Aff{x, y});
+  XYZZ d1 = p1.dbl();
+  XYZZ s1 = p1;
+  s1.add(p1);
+  res[7 * i + 6] = (d1.X == s1.X && d1.Y == s1.Y && d1.ZZ == s1.ZZ && d1.ZZZ == s1.ZZZ) ? Fq::one() : Fq::zero();
+}
+
+
+__global__ void k_echo(Fr a, uint64_t pad, Fr b, int flag, Fr* out, const Fr* pa) {
+  if (threadIdx.x != 0 || blockIdx.x != 0) return;
+  out[0] = a;
+  out[1] = b;
+  out[2] = a * b;
+  out[3] = pa[0] * pa[1];
+  out[4] = pa[0];
+  Fr c = pa[1];
+  out[5] = a * c;
+  out[6] = c * a;
+  out[7] = Fr::mul(pa[1], a);
+  (void)pad; (void)flag;
+}
+
+}  // namespace
+
+extern "C" {
+
+const char* zg_last_error(void) { return g_err.c_str(); }
+
+int zg_ctx_create(const zg_config* cfg, zg_ctx** out) {
+  if (!cfg || !out) return fail(ZG_ERR_INVALID_ARG, "null argument");
+  if (cfg->log_row < 1 || cfg->log_col < 3 || cfg->log_row > 11 || cfg->log_col > 11)
+    return fail(ZG_ERR_INVALID_ARG, "log_row must be in [1, 11] and log_col in [3, 11]");
+  zg_ctx* c = new zg_ctx();
+  *out = nullptr;
+  c->device = cfg->device;
+  c->lr = (int)cfg->log_row;
+  c->lc = (int)cfg->log_col;
+  c->L = c->lr + 2;
+  c->R = size_t(1) << c->lr;
+  c->C = size_t(1) << c->lc;
+  c->N = c->R * c->C;
+  c->max_blob = 31 * c->N;
+  c->max_raw = c->max_blob - 4;
+  int rc = 0;
+  auto bail = [&](int code) {
+    zg_ctx_destroy(c);
+    return code;
+  };
+  if (cudaSetDevice(c->device) != cudaSuccess) return bail(fail(ZG_ERR_CUDA, "cudaSetDevice failed"));
+  if ((rc = set_smem_limits())) return bail(rc);
+  if (cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking) != cudaSuccess)
+    return bail(fail(ZG_ERR_CUDA, "stream create failed"));
+  if ((rc = make_twiddles(c->lr, c->lc, &c->tw))) return bail(rc);
+  if (cudaMalloc(&c->bases, (size_t)3 * c->L * c->N * sizeof(G1Aff)) != cudaSuccess)
+    return bail(fail(ZG_ERR_CUDA, "cannot allocate params"));
+  if ((rc = alloc_blob_buffers(c))) return bail(rc);
+  if (cfg->params_dir && cfg->params_dir[0]) rc = load_mont_params(c, cfg->params_dir);
+  else rc = build_seeded_params(c, cfg->tau_seed);
+  if (rc) return bail(rc);
+  *out = c;
+  return ZG_OK;
+}
+
+void zg_ctx_destroy(zg_ctx* c) {
+  if (!c) return;
+  cudaSetDevice(c->device);
+  if (c->stream) cudaStreamSynchronize(c->stream);
+  free_twiddles(&c->tw);
+  void* ps[] = {c->bases, c->raw, c->enc, c->T1, c->Bc, c->win, c->part, c->nodes, c->amt,
+                c->tree, c->tree_off_d, c->slices, c->file_root};
+  for (void* p : ps) if (p) cudaFree(p);
+  if (c->h_in) cudaFreeHost(c->h_in);
+  if (c->stream) cudaStreamDestroy(c->stream);
+  delete c;
+}
+
+int zg_encode_device(zg_ctx* c, const void* d_data, size_t len, void* stream, zg_device_blob* out) {
+  if (!c || !out || (!d_data && len)) return fail(ZG_ERR_INVALID_ARG, "null argument");
+  if (len > c->max_raw) {
+    char m[128];
+    snprintf(m, sizeof(m), "TooLargeBlob { actual: %zu, expected_max: %zu }", len, c->max_raw);
+    return fail(ZG_ERR_TOO_LARGE_BLOB, m);
+  }
+  std::lock_guard<std::mutex> g(c->mu);
+  if (cudaSetDevice(c->device) != cudaSuccess) return fail(ZG_ERR_CUDA, "cudaSetDevice failed");
+  cudaStream_t s = stream ? (cudaStream_t)stream : c->stream;
+  int rc = encode_device_locked(c, (const uint8_t*)d_data, len, s);
+  if (rc) return rc;
+  out->encoded_data = c->enc;
+  out->slices = c->slices;
+  out->slice_size = c->slice_size;
+  out->amt_outputs = c->amt;
+  out->roots = c->tree + c->tree_off[0];
+  out->file_root = c->file_root;
+  return ZG_OK;
+}
+
+int zg_encode(zg_ctx* c, const uint8_t* data, size_t len, int require_data, zg_reply** out) {
+  if (!c || !out || (!data && len)) return fail(ZG_ERR_INVALID_ARG, "null argument");
+  *out = nullptr;
+  if (len > c->max_raw) {  // RawData::try_from (crates/encoder/src/raw_data.rs:76-95)
+    char m[128];
+    snprintf(m, sizeof(m), "TooLargeBlob { actual: %zu, expected_max: %zu }", len, c->max_raw);
+    return fail(ZG_ERR_TOO_LARGE_BLOB, m);
+  }
+  std::lock_guard<std::mutex> g(c->mu);
+  if (cudaSetDevice(c->device) != cudaSuccess) return fail(ZG_ERR_CUDA, "cudaSetDevice failed");
+  cudaStream_t s = c->stream;
+  zg_reply* r = new zg_reply();
+  auto bail = [&](int code) {
+    zg_reply_free(r);
+    return code;
+  };
+  r->slice_size = c->slice_size;
+  r->nslices = 3 * c->R;
+  if (cudaMallocHost(&r->slices, r->nslices * r->slice_size) != cudaSuccess)
+    return bail(fail(ZG_ERR_CUDA, "cannot allocate pinned reply"));
+  if (require_data) {
+    r->data_len = 3 * c->N * 32;
+    if (cudaMallocHost(&r->data, r->data_len) != cudaSuccess)
+      return bail(fail(ZG_ERR_CUDA, "cannot allocate pinned reply"));
+  }
+  if (len) memcpy(c->h_in, data, len);
+  if (len && cudaMemcpyAsync(c->raw, c->h_in, len, cudaMemcpyHostToDevice, s) != cudaSuccess)
+    return bail(fail(ZG_ERR_CUDA, "H2D copy failed"));
+  int rc = encode_device_locked(c, c->raw, len, s);
+  if (rc) return bail(rc);
+  uint8_t amt_roots[3][64];
+  bool ok = true;
+  for (int cs = 0; cs < 3 && ok; ++cs)
+    ok = cudaMemcpyAsync(amt_roots[cs], c->amt + (size_t)cs * (4 * c->R - 2) * 64, 64, cudaMemcpyDeviceToHost, s) ==
+         cudaSuccess;
+  ok = ok && cudaMemcpyAsync(r->roots, c->tree + c->tree_off[0], 96, cudaMemcpyDeviceToHost, s) == cudaSuccess;
+  ok = ok && cudaMemcpyAsync(r->storage_root, c->file_root, 32, cudaMemcpyDeviceToHost, s) == cudaSuccess;
+  ok = ok && cudaMemcpyAsync(r->slices, c->slices, r->nslices * r->slice_size, cudaMemcpyDeviceToHost, s) ==
+             cudaSuccess;
+  if (require_data)
+    ok = ok && cudaMemcpyAsync(r->data, c->enc, r->data_len, cudaMemcpyDeviceToHost, s) == cudaSuccess;
+  if (!ok) return bail(fail(ZG_ERR_CUDA, "D2H copy failed"));
+  cudaError_t e = cudaStreamSynchronize(s);
+  if (e != cudaSuccess) return bail(fail(ZG_ERR_CUDA, std::string("encode: ") + cudaGetErrorString(e)));
+  // EncodedBlobAMT::assert_commitment_consistent (crates/encoder/src/amt/blob.rs:42-47)
+  if (memcmp(amt_roots[0], amt_roots[1], 64) || memcmp(amt_roots[0], amt_roots[2], 64))
+    return bail(fail(ZG_ERR_INTERNAL, "coset commitments differ"));
+  // erasure_commitment = x || y canonical without flags (grpc/src/service.rs:77-83)
+  if (amt_roots[0][63] & 0x40) {
+    memset(r->commitment, 0, 64);
+  } else {
+    memcpy(r->commitment, amt_roots[0], 64);
+    r->commitment[63] &= 0x3f;
+  }
+  *out = r;
+  return ZG_OK;
+}
+
+int zg_ctx_warmup(zg_ctx* c) {
+  zg_reply* r = nullptr;
+  int rc = zg_encode(c, nullptr, 0, 1, &r);
+  zg_reply_free(r);
+  return rc;
+}
+
+void zg_reply_free(zg_reply* r) {
+  if (!r) return;
+  if (r->slices) cudaFreeHost(r->slices);
+  if (r->data) cudaFreeHost(r->data);
+  delete r;
+}
+uint32_t zg_reply_version(const zg_reply* r) { return r->version; }
+const uint8_t* zg_reply_erasure_commitment(const zg_reply* r, size_t* len) {
+  if (len) *len = 64;
+  return r->commitment;
+}
+const uint8_t* zg_reply_storage_root(const zg_reply* r, size_t* len) {
+  if (len) *len = 32;
+  return r->storage_root;
+}
+const uint8_t* zg_reply_encoded_data(const zg_reply* r, size_t* len) {
+  if (len) *len = r->data_len;
+  return r->data;
+}
+size_t zg_reply_num_slices(const zg_reply* r) { return r->nslices; }
+const uint8_t* zg_reply_slice(const zg_reply* r, size_t index, size_t* len) {
+  if (index >= r->nslices) {
+    if (len) *len = 0;
+    return nullptr;
+  }
+  if (len) *len = r->slice_size;
+  return r->slices + index * r->slice_size;
+}
+const uint8_t* zg_reply_roots(const zg_reply* r, size_t* len) {
+  if (len) *len = 96;
+  return r->roots;
+}
+
+int zg_ctx_param_line(zg_ctx* c, int coset, int line, uint8_t* host_out, size_t cap) {
+  if (!c || coset < 0 || coset > 2 || line < 0 || line >= c->L) return fail(ZG_ERR_INVALID_ARG, "bad line");
+  size_t bytes = c->N * sizeof(G1Aff);
+  if (cap < bytes) return fail(ZG_ERR_INVALID_ARG, "buffer too small");
+  std::lock_guard<std::mutex> g(c->mu);
+  ZG_CK(cudaSetDevice(c->device));
+  ZG_CK(cudaMemcpy(host_out, c->bases + ((size_t)coset * c->L + line) * c->N, bytes, cudaMemcpyDeviceToHost));
+  return ZG_OK;
+}
+
+int zg_msm_chunks(const void* d_bases, const void* d_scalars, uint32_t lines, uint32_t log_nchunks,
+                  uint32_t log_chunk, void* d_out, void* stream) {
+  if (!d_bases || !d_scalars || !d_out || lines == 0 || log_chunk > 10 || log_nchunks > 20)
+    return fail(ZG_ERR_INVALID_ARG, "bad msm arguments");
+  int rc = set_smem_limits();
+  if (rc) return rc;
+  cudaStream_t s = (cudaStream_t)stream;
+  const size_t nch = size_t(1) << log_nchunks;
+  const size_t count = (size_t)lines * nch;
+  XYZZ *win = nullptr, *part = nullptr;
+  ZG_CK(cudaMallocAsync(&win, count * MSM_WINDOWS * sizeof(XYZZ), s));
+  ZG_CK(cudaMallocAsync(&part, count * sizeof(XYZZ), s));
+  MsmChunkArgs a;
+  a.scalars = (const uint8_t*)d_scalars;
+  a.bases = (const G1Aff*)d_bases;
+  a.win = win;
+  a.lr = (int)log_nchunks;
+  a.lc = (int)log_chunk;
+  a.lines = (int)lines;
+  a.bitrev_rows = 0;
+  a.scalar_coset_stride = 0;
+  a.base_coset_stride = 0;
+  k_msm_chunks<<<dim3((unsigned)nch, 1), MSM_THREADS, msm_smem_bytes((int)log_chunk), s>>>(a);
+  k_msm_combine<<<nblk(count, 64), 64, 0, s>>>(win, part, (uint32_t)count);
+  k_serialize_nodes<<<nblk(count, 128), 128, 0, s>>>(part, (uint8_t*)d_out, (uint32_t)count);
+  rc = check_launch();
+  cudaFreeAsync(win, s);
+  cudaFreeAsync(part, s);
+  return rc;
+}
+
+int zg_ntt(void* d_data, uint32_t log_n, uint32_t batch, int inverse, uint32_t coset_idx, void* stream) {
+  if (!d_data || log_n < 1 || log_n > 22 || batch == 0) return fail(ZG_ERR_INVALID_ARG, "bad ntt arguments");
+  if (coset_idx && inverse) return fail(ZG_ERR_INVALID_ARG, "coset shift is forward-only");
+  int rc = set_smem_limits();
+  if (rc) return rc;
+  cudaStream_t s = (cudaStream_t)stream;
+  ZG_CK(cudaFuncSetAttribute(k_ntt_small, cudaFuncAttributeMaxDynamicSharedMemorySize, 227 * 1024));
+  const size_t n = size_t(1) << log_n;
+  Fr* v = (Fr*)d_data;
+  const unsigned T = 256;
+  Fr g = coset_idx ? coset_factor((int)log_n, coset_idx) : Fr::one();
+  Fr ninv = host_fr_from_u32((uint32_t)n).inverse();
+  const uint64_t total = (uint64_t)batch * n;
+  k_canon_to_mont<<<nblk(total, T), T, 0, s>>>(v, total, (int)log_n, g, coset_idx ? 1 : 0);
+  if (log_n <= 11) {
+    const Twiddles* tw = cached_twiddles(0, (int)log_n);
+    if (!tw) return ZG_ERR_CUDA;
+    for (uint32_t b0 = 0; b0 < batch;) {
+      uint32_t nb = std::min<uint32_t>(batch - b0, 65535);
+      k_ntt_small<<<nb, 256, n * sizeof(Fr), s>>>(v + (size_t)b0 * n, (int)log_n, inverse ? tw->twi_c : tw->twf_c);
+      b0 += nb;
+    }
+  } else {
+    const int lc = (int)(log_n + 1) / 2, lr = (int)log_n - lc;
+    const Twiddles* tw = cached_twiddles(lr, lc);
+    if (!tw) return ZG_ERR_CUDA;
+    Fr* tmp = nullptr;
+    ZG_CK(cudaMallocAsync(&tmp, n * sizeof(Fr), s));
+    for (uint32_t b = 0; b < batch; ++b) ntt4(*tw, v + (size_t)b * n, tmp, v + (size_t)b * n, inverse != 0, s);
+    cudaFreeAsync(tmp, s);
+  }
+  k_mont_to_canon<<<nblk(total, T), T, 0, s>>>(v, total, ninv, inverse ? 1 : 0);
+  return check_launch();
+}
+
+
+int zg_selftest(int* fails, int nops) {
+  const uint32_t n = 1024;
+  std::vector<Fq> a(n), b(n);
+  uint64_t st = 0x1234;
+  for (uint32_t i = 0; i < n; ++i) {
+    for (int k = 0; k < 8; ++k) {
+      a[i].v[k] = (uint32_t)splitmix64(st);
+      b[i].v[k] = (uint32_t)splitmix64(st);
+    }
+    // full-range operands below the Fr modulus (so they are valid for both fields)
+    a[i].v[7] &= 0x3fffffffu;
+    b[i].v[7] &= 0x3fffffffu;
+    if (i & 1) { a[i].v[7] &= 0x0fffffffu; b[i].v[7] &= 0x0fffffffu; }
+    for (Fq* x : {&a[i], &b[i]}) {
+      Fr t = *reinterpret_cast<Fr*>(x);
+      for (;;) {
+        Fr d;
+        if (Fr::sub_raw(d, t, Fr::modulus())) break;
+        t = d;
+      }
+      *x = *reinterpret_cast<Fq*>(&t);
+    }
+  }
+  Fq *da = nullptr, *db = nullptr, *dr = nullptr;
+  ZG_CK(cudaMalloc(&da, n * sizeof(Fq)));
+  ZG_CK(cudaMalloc(&db, n * sizeof(Fq)));
+  ZG_CK(cudaMalloc(&dr, 7 * n * sizeof(Fq)));
+  ZG_CK(cudaMemcpy(da, a.data(), n * sizeof(Fq), cudaMemcpyHostToDevice));
+  ZG_CK(cudaMemcpy(db, b.data(), n * sizeof(Fq), cudaMemcpyHostToDevice));
+  k_selftest<<<n / 128, 128>>>(da, db, dr, n);
+  ZG_CK(cudaDeviceSynchronize());
+  std::vector<Fq> r(7 * n);
+  ZG_CK(cudaMemcpy(r.data(), dr, 7 * n * sizeof(Fq), cudaMemcpyDeviceToHost));
+  cudaFree(da); cudaFree(db); cudaFree(dr);
+  int cnt[7] = {0, 0, 0, 0, 0, 0, 0};
+  for (uint32_t i = 0; i < n; ++i) {
+    Fq x = a[i], y = b[i];
+    Fq e[7];
+    e[0] = Fq::mul(x, y);
+    e[1] = e[0];
+    e[2] = Fq::add(x, y);
+    e[3] = Fq::sub(x, y);
+    Fr xr = *reinterpret_cast<const Fr*>(&x), yr = *reinterpret_cast<const Fr*>(&y);
+    Fr m = Fr::mul(xr, yr);
+    e[4] = *reinterpret_cast<Fq*>(&m);
+    e[5] = *reinterpret_cast<Fq*>(&xr);
+    e[6] = Fq::one();
+    for (int k = 0; k < 7; ++k) cnt[k] += (r[7 * i + k] != e[k]);
+  }
+  for (int k = 0; k < nops && k < 7; ++k) fails[k] = cnt[k];
+  return ZG_OK;
+}
+
+
+int zg_debug_echo(uint8_t* host_out) {  // host_out: 11 x 32 B
+  Fr a = host_fr_from_u32(32).inverse(), b = coset_factor(5, 1);
+  Fr* d = nullptr;
+  ZG_CK(cudaMalloc(&d, 16 * sizeof(Fr)));
+  Fr ab[2] = {a, b};
+  ZG_CK(cudaMemcpy(d + 12, ab, 2 * sizeof(Fr), cudaMemcpyHostToDevice));
+  k_echo<<<1, 32>>>(a, 77, b, 1, d, d + 12);
+  // k_mont_to_canon on [b, b] with scale a
+  ZG_CK(cudaMemcpy(d + 8, ab + 1, sizeof(Fr), cudaMemcpyHostToDevice));
+  ZG_CK(cudaMemcpy(d + 9, ab + 1, sizeof(Fr), cudaMemcpyHostToDevice));
+  k_mont_to_canon<<<1, 32>>>(d + 8, 2, a, 1);
+  ZG_CK(cudaDeviceSynchronize());
+  ZG_CK(cudaMemcpy(host_out, d, 10 * sizeof(Fr), cudaMemcpyDeviceToHost));
+  Fr ref = (b * a).to_canonical();
+  memcpy(host_out + 10 * 32, &ref, 32);
+  cudaFree(d);
+  return 0;
+}
+
+int zg_merkle_roots(const void* d_items, size_t n_items, void* d_roots, void* stream) {
+  if (!d_items || !d_roots || n_items < 24 || n_items % 24) return fail(ZG_ERR_INVALID_ARG, "n_items must be 3*8*2^k");
+  size_t leaves = n_items / 8;
+  size_t per = leaves / 3;
+  if (per & (per - 1)) return fail(ZG_ERR_INVALID_ARG, "n_items must be 3*8*2^k");
+  int depth = 0;
+  while (((size_t)3 << depth) < leaves) ++depth;
+  std::vector<uint64_t> off(depth + 1);
+  size_t o = 0;
+  for (int d = 0; d <= depth; ++d) {
+    off[d] = o;
+    o += ((size_t)3 << d) * 32;
+  }
+  cudaStream_t s = (cudaStream_t)stream;
+  uint8_t* tree = nullptr;
+  ZG_CK(cudaMallocAsync(&tree, o, s));
+  int rc = merkle_levels((const uint8_t*)d_items, n_items, tree, off, depth, s);
+  if (!rc) ZG_CK(cudaMemcpyAsync(d_roots, tree, 96, cudaMemcpyDeviceToDevice, s));
+  cudaFreeAsync(tree, s);
+  return rc;
+}
+
+}  // extern "C"

@@ -1,0 +1,637 @@
+// Device kernels of the blob-encoding path.
+//
+// Layout in HBM for one blob of R = 2^LR rows and C = 2^LC columns
+// (N = R*C scalars; production R = C = 1024):
+//   enc   [3][R][C] x 32 B   encoded rows, canonical little-endian Fr, coset-
+//                             major then row-major: the reference's
+//                             EncodedBlob::get_data() order (amt/blob.rs:29-40)
+//   T1    [R][C]   Fr(mont)  row-iNTT output of the original rows
+//   Bc    [2][R][C] Fr(mont) column pass output for cosets 1, 2 (transposed)
+//   bases [3][L][N] G1 affine (Montgomery x||y, 64 B), L = LR + 2 lines in the
+//                             order quotients[0..LR), basis, high_basis (the
+//                             upload order of prove_gpu.rs:42-47)
+//   win   [3][L][R][32] XYZZ  per-chunk MSM window sums
+//   amt   [3][4R-2] 64 B     AMT outputs, ark uncompressed G1
+//   tree  levels of the Merkle tree (level d holds 3*2^d nodes)
+#pragma once
+#include <stdint.h>
+
+#include "zg_curve.cuh"
+#include "zg_keccak.cuh"
+
+namespace zg {
+
+__device__ __forceinline__ uint32_t brev_bits(uint32_t x, int bits) {
+  return bits == 0 ? 0u : (__brev(x) >> (32 - bits));
+}
+
+// ---------------------------------------------------------------------------
+// shared-memory radix-2 DIT NTT; s[] holds the input in bit-reversed order,
+// tw[k] = w^k for k < n/2 of the n-th root in use. Result in natural order.
+__device__ __forceinline__ void ntt_smem(Fr* s, int logn, const Fr* __restrict__ tw) {
+  const int n = 1 << logn;
+  for (int st = 1; st <= logn; ++st) {
+    const int half = 1 << (st - 1);
+    const int stride = n >> st;
+    for (int bf = threadIdx.x; bf < (n >> 1); bf += blockDim.x) {
+      int k = bf & (half - 1);
+      int i = ((bf >> (st - 1)) << st) + k;
+      Fr w = tw[k * stride];
+      Fr u = s[i];
+      Fr v = s[i + half] * w;
+      s[i] = u + v;
+      s[i + half] = u - v;
+    }
+    __syncthreads();
+  }
+}
+
+__device__ __forceinline__ Fr load_fr(const Fr* p) {
+  const uint4* q = reinterpret_cast<const uint4*>(p);
+  uint4 a = q[0], b = q[1];
+  Fr r;
+  r.v[0] = a.x; r.v[1] = a.y; r.v[2] = a.z; r.v[3] = a.w;
+  r.v[4] = b.x; r.v[5] = b.y; r.v[6] = b.z; r.v[7] = b.w;
+  return r;
+}
+__device__ __forceinline__ void store_fr(Fr* p, const Fr& x) {
+  uint4* q = reinterpret_cast<uint4*>(p);
+  q[0] = make_uint4(x.v[0], x.v[1], x.v[2], x.v[3]);
+  q[1] = make_uint4(x.v[4], x.v[5], x.v[6], x.v[7]);
+}
+
+// w_N^e from the split tables lo[e & (C-1)] * hi[e >> LC]
+__device__ __forceinline__ Fr pow_split(const Fr* lo, const Fr* hi, uint32_t e, int lc, uint32_t nmask) {
+  e &= nmask;
+  return lo[e & ((1u << lc) - 1)] * hi[e >> lc];
+}
+
+// Pass 1: original row r -> canonical enc[0][r][*], and
+// T1[r][s] = w_N^{-s r} * sum_j v_C^{-s j} D[r][j]   (Montgomery).
+// D[r][j] is the Fr of the 31-byte chunk r*C + j of the zero-padded RawData
+// whose last four bytes hold the payload length (raw_data.rs:55-73,
+// raw_blob.rs:33-40).
+__global__ void k_rows_from_raw(const uint8_t* __restrict__ raw, uint64_t len, uint64_t max_raw, int lr, int lc,
+                                uint8_t* __restrict__ enc0, Fr* __restrict__ T1, const Fr* __restrict__ twi_c,
+                                const Fr* __restrict__ wni_lo, const Fr* __restrict__ wni_hi) {
+  extern __shared__ __align__(16) uint8_t smem[];
+  const int C = 1 << lc;
+  const uint32_t r = blockIdx.x;
+  Fr* s = reinterpret_cast<Fr*>(smem);
+  uint8_t* bytes = smem + (size_t)C * sizeof(Fr);
+  const uint64_t base = (uint64_t)31 * r * C;
+  const uint32_t nbytes = 31u * C;
+  for (uint32_t i = threadIdx.x; i < nbytes; i += blockDim.x) {
+    uint64_t o = base + i;
+    uint8_t v = 0;
+    if (o < len) v = raw[o];
+    else if (o >= max_raw) v = (uint8_t)(len >> (8 * (o - max_raw)));
+    bytes[i] = v;
+  }
+  __syncthreads();
+  for (int j = threadIdx.x; j < C; j += blockDim.x) {
+    Fr x;
+    const uint8_t* b = bytes + 31 * j;
+#pragma unroll
+    for (int k = 0; k < 8; ++k) {
+      uint32_t w = 0;
+#pragma unroll
+      for (int t = 0; t < 4; ++t) {
+        int idx = 4 * k + t;
+        if (idx < 31) w |= (uint32_t)b[idx] << (8 * t);
+      }
+      x.v[k] = w;
+    }
+    store_fr(reinterpret_cast<Fr*>(enc0) + ((size_t)r * C + j), x);
+    s[brev_bits(j, lc)] = Fr::from_canonical(x);
+  }
+  __syncthreads();
+  ntt_smem(s, lc, twi_c);
+  const uint32_t nmask = (1u << (lr + lc)) - 1;
+  for (int k = threadIdx.x; k < C; k += blockDim.x) {
+    Fr t = s[k] * pow_split(wni_lo, wni_hi, (uint32_t)k * r, lc, nmask);
+    store_fr(T1 + (size_t)r * C + k, t);
+  }
+}
+
+// Pass 2: per column s, iNTT over rows (size R), then per extension coset
+// c in {1, 2}: scale coefficient m = s + C q by g_c^m / N, forward NTT over q,
+// multiply by w_N^{s r}; store Bc[c-1][r][s].
+constexpr int COLS_PER_BLOCK = 2;
+__global__ void k_cols(const Fr* __restrict__ T1, Fr* __restrict__ Bc, int lr, int lc,
+                       const Fr* __restrict__ twi_r, const Fr* __restrict__ twf_r,
+                       const Fr* __restrict__ gs_lo, const Fr* __restrict__ gs_hi,
+                       const Fr* __restrict__ wn_lo, const Fr* __restrict__ wn_hi) {
+  extern __shared__ __align__(16) uint8_t smem[];
+  const int R = 1 << lr, C = 1 << lc;
+  Fr* coef = reinterpret_cast<Fr*>(smem);
+  Fr* work = coef + (size_t)R;
+  const uint32_t nmask = (1u << (lr + lc)) - 1;
+  for (int cc = 0; cc < COLS_PER_BLOCK; ++cc) {
+    const uint32_t s = blockIdx.x * COLS_PER_BLOCK + cc;
+    if (s >= (uint32_t)C) break;
+    for (int r = threadIdx.x; r < R; r += blockDim.x)
+      coef[brev_bits(r, lr)] = load_fr(T1 + (size_t)r * C + s);
+    __syncthreads();
+    ntt_smem(coef, lr, twi_r);
+    for (int c = 0; c < 2; ++c) {
+      const Fr glo = gs_lo[c * C + s];
+      for (int q = threadIdx.x; q < R; q += blockDim.x)
+        work[brev_bits(q, lr)] = coef[q] * glo * gs_hi[c * R + q];
+      __syncthreads();
+      ntt_smem(work, lr, twf_r);
+      for (int r = threadIdx.x; r < R; r += blockDim.x) {
+        Fr t = work[r] * pow_split(wn_lo, wn_hi, s * (uint32_t)r, lc, nmask);
+        store_fr(Bc + ((size_t)c * R + r) * C + s, t);
+      }
+      __syncthreads();
+    }
+  }
+}
+
+// Pass 3: per coset c in {1,2} and row r, forward NTT over s (size C):
+// enc[c][r][j] = canonical( sum_s v_C^{s j} Bc[c-1][r][s] ).
+__global__ void k_rows_ntt(const Fr* __restrict__ Bc, uint8_t* __restrict__ enc, int lr, int lc,
+                           const Fr* __restrict__ twf_c) {
+  extern __shared__ __align__(16) uint8_t smem[];
+  const int R = 1 << lr, C = 1 << lc;
+  const uint32_t r = blockIdx.x, c = blockIdx.y;
+  Fr* s = reinterpret_cast<Fr*>(smem);
+  const Fr* src = Bc + ((size_t)c * R + r) * C;
+  for (int k = threadIdx.x; k < C; k += blockDim.x) s[brev_bits(k, lc)] = load_fr(src + k);
+  __syncthreads();
+  ntt_smem(s, lc, twf_c);
+  Fr* dst = reinterpret_cast<Fr*>(enc) + ((size_t)(c + 1) * R + r) * C;
+  for (int j = threadIdx.x; j < C; j += blockDim.x) store_fr(dst + j, s[j].to_canonical());
+}
+
+// ---------------------------------------------------------------------------
+// MSM over per-row chunks (the decomposition of prove_gpu.rs:55-87: for every
+// line l and chunk b, the MSM of the C scalars of chunk b against
+// bases[l][b*C .. (b+1)*C)). Chunk b of the bit-reversed coset vector is
+// encoded row bitrev(b), element t is column bitrev(t)
+// (HalfBlob::generate, crates/amt/src/blob/encode.rs:171-183).
+//
+// Signed 8-bit windows: 32 windows, digits in [-128, 127], buckets 1..128.
+// One CTA per (chunk, coset): the digits of the chunk's C scalars are
+// counting-sorted into per-window bucket lists once and reused for all L
+// lines. Thread (line li, window w, segment g) owns buckets 64g+1..64g+64 of
+// one window: it sums each bucket from the affine bases and folds it into
+// running sums, so no bucket array is materialised; the two segments of a
+// window meet through a warp shuffle.
+constexpr int MSM_WINDOWS = 32;
+constexpr int MSM_THREADS = 256;
+constexpr int MSM_LINES_PER_PASS = MSM_THREADS / (MSM_WINDOWS * 2);
+
+__device__ __forceinline__ XYZZ shfl_down_xyzz(const XYZZ& p, int delta) {
+  XYZZ r;
+#pragma unroll
+  for (int i = 0; i < 8; ++i) {
+    r.X.v[i] = __shfl_down_sync(0xffffffffu, p.X.v[i], delta);
+    r.Y.v[i] = __shfl_down_sync(0xffffffffu, p.Y.v[i], delta);
+    r.ZZ.v[i] = __shfl_down_sync(0xffffffffu, p.ZZ.v[i], delta);
+    r.ZZZ.v[i] = __shfl_down_sync(0xffffffffu, p.ZZZ.v[i], delta);
+  }
+  return r;
+}
+
+__device__ __forceinline__ G1Aff load_aff(const G1Aff* p) {
+  const uint4* q = reinterpret_cast<const uint4*>(p);
+  uint4 a = __ldg(q), b = __ldg(q + 1), c = __ldg(q + 2), d = __ldg(q + 3);
+  G1Aff r;
+  r.x.v[0] = a.x; r.x.v[1] = a.y; r.x.v[2] = a.z; r.x.v[3] = a.w;
+  r.x.v[4] = b.x; r.x.v[5] = b.y; r.x.v[6] = b.z; r.x.v[7] = b.w;
+  r.y.v[0] = c.x; r.y.v[1] = c.y; r.y.v[2] = c.z; r.y.v[3] = c.w;
+  r.y.v[4] = d.x; r.y.v[5] = d.y; r.y.v[6] = d.z; r.y.v[7] = d.w;
+  return r;
+}
+
+__device__ __forceinline__ void store_xyzz(XYZZ* p, const XYZZ& x) {
+  store_fr(reinterpret_cast<Fr*>(&p->X), *reinterpret_cast<const Fr*>(&x.X));
+  store_fr(reinterpret_cast<Fr*>(&p->Y), *reinterpret_cast<const Fr*>(&x.Y));
+  store_fr(reinterpret_cast<Fr*>(&p->ZZ), *reinterpret_cast<const Fr*>(&x.ZZ));
+  store_fr(reinterpret_cast<Fr*>(&p->ZZZ), *reinterpret_cast<const Fr*>(&x.ZZZ));
+}
+__device__ __forceinline__ XYZZ load_xyzz(const XYZZ* p) {
+  XYZZ r;
+  Fr a = load_fr(reinterpret_cast<const Fr*>(&p->X));
+  Fr b = load_fr(reinterpret_cast<const Fr*>(&p->Y));
+  Fr c = load_fr(reinterpret_cast<const Fr*>(&p->ZZ));
+  Fr d = load_fr(reinterpret_cast<const Fr*>(&p->ZZZ));
+#pragma unroll
+  for (int i = 0; i < 8; ++i) {
+    r.X.v[i] = a.v[i]; r.Y.v[i] = b.v[i]; r.ZZ.v[i] = c.v[i]; r.ZZZ.v[i] = d.v[i];
+  }
+  return r;
+}
+
+struct MsmChunkArgs {
+  const uint8_t* scalars;  // canonical 32 B scalars
+  const G1Aff* bases;      // [cosets][L][N]
+  XYZZ* win;               // [cosets][L][nchunks][32]
+  int lr, lc;              // nchunks = 2^lr, chunk = 2^lc
+  int lines;               // L
+  int bitrev_rows;         // 1: chunk b reads encoded row bitrev(b), column bitrev(t)
+  uint64_t scalar_coset_stride;  // scalars between cosets (elements)
+  uint64_t base_coset_stride;    // bases between cosets (points)
+};
+
+__global__ void __launch_bounds__(MSM_THREADS, 1) k_msm_chunks(MsmChunkArgs a) {
+  extern __shared__ __align__(16) uint8_t smem[];
+  const int C = 1 << a.lc;
+  const int N = 1 << (a.lr + a.lc);
+  const uint32_t b = blockIdx.x, coset = blockIdx.y;
+  // smem: scalars [C][8] u32 | lists [32][C] u16 | offs [32][129] u16 | cnt [129] u32
+  uint32_t* scal = reinterpret_cast<uint32_t*>(smem);
+  uint16_t* lists = reinterpret_cast<uint16_t*>(scal + (size_t)C * 8);
+  uint16_t* offs = lists + (size_t)MSM_WINDOWS * C;
+  uint32_t* cnt = reinterpret_cast<uint32_t*>(offs + MSM_WINDOWS * 129 + (MSM_WINDOWS * 129) % 2);
+
+  const uint32_t row = a.bitrev_rows ? brev_bits(b, a.lr) : b;
+  const uint8_t* src = a.scalars + (a.scalar_coset_stride * coset + (uint64_t)row * C) * 32;
+  for (int t = threadIdx.x; t < C; t += blockDim.x) {
+    uint32_t col = a.bitrev_rows ? brev_bits(t, a.lc) : t;
+    const uint4* q = reinterpret_cast<const uint4*>(src + (size_t)col * 32);
+    uint4 x = q[0], y = q[1];
+    uint32_t* d = scal + (size_t)t * 8;
+    d[0] = x.x; d[1] = x.y; d[2] = x.z; d[3] = x.w; d[4] = y.x; d[5] = y.y; d[6] = y.z; d[7] = y.w;
+  }
+  __syncthreads();
+
+  // signed-digit decomposition + per-window counting sort
+  constexpr int MAXPER = 8;  // supports C <= 2048
+  uint32_t carry_bits = 0;   // bit i: carry of this thread's i-th scalar
+  for (int w = 0; w < MSM_WINDOWS; ++w) {
+    for (int k = threadIdx.x; k <= 128; k += blockDim.x) cnt[k] = 0;
+    __syncthreads();
+    int digs[MAXPER];
+#pragma unroll
+    for (int i = 0; i < MAXPER; ++i) {
+      int t = threadIdx.x + i * blockDim.x;
+      digs[i] = 0;
+      if (t < C) {
+        uint32_t byte = (scal[(size_t)t * 8 + (w >> 2)] >> (8 * (w & 3))) & 0xff;
+        uint32_t v = byte + ((carry_bits >> i) & 1);
+        int d;
+        if (v >= 128) { d = (int)v - 256; carry_bits |= 1u << i; }
+        else { d = (int)v; carry_bits &= ~(1u << i); }
+        digs[i] = d;
+        if (d) atomicAdd(&cnt[d < 0 ? -d : d], 1u);
+      }
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      uint32_t acc = 0;
+      for (int k = 1; k <= 128; ++k) {
+        offs[w * 129 + k - 1] = (uint16_t)acc;
+        uint32_t c = cnt[k];
+        cnt[k] = acc;
+        acc += c;
+      }
+      offs[w * 129 + 128] = (uint16_t)acc;
+    }
+    __syncthreads();
+#pragma unroll
+    for (int i = 0; i < MAXPER; ++i) {
+      int t = threadIdx.x + i * blockDim.x;
+      int d = digs[i];
+      if (t < C && d) {
+        uint32_t k = d < 0 ? -d : d;
+        uint32_t pos = atomicAdd(&cnt[k], 1u);
+        lists[(size_t)w * C + pos] = (uint16_t)(t | (d < 0 ? 0x8000 : 0));
+      }
+    }
+    __syncthreads();
+  }
+
+  // bucket accumulation + window reduction
+  const int li = threadIdx.x / (MSM_WINDOWS * 2);
+  const int w = (threadIdx.x / 2) % MSM_WINDOWS;
+  const int g = threadIdx.x & 1;
+  const int nchunks = 1 << a.lr;
+  for (int l0 = 0; l0 < a.lines; l0 += MSM_LINES_PER_PASS) {
+    const int l = l0 + li;
+    const bool active = l < a.lines;
+    const G1Aff* bl = a.bases + a.base_coset_stride * coset + (size_t)(active ? l : 0) * N + (size_t)b * C;
+    XYZZ run = XYZZ::inf(), acc = XYZZ::inf();
+    if (active) {
+      for (int k = 64 * g + 64; k > 64 * g; --k) {
+        XYZZ bucket = XYZZ::inf();
+        const int beg = offs[w * 129 + k - 1], end = offs[w * 129 + k];
+        for (int e = beg; e < end; ++e) {
+          uint32_t ent = lists[(size_t)w * C + e];
+          G1Aff p = load_aff(bl + (ent & 0x7fff));
+          if (ent & 0x8000) p.y = -p.y;
+          bucket.add_affine(p.x, p.y);
+        }
+        run.add(bucket);
+        acc.add(run);
+      }
+    }
+    // window = acc0 + acc1 + 64 * run1   (segment 1 holds buckets 65..128)
+    XYZZ acc1 = shfl_down_xyzz(acc, 1);
+    XYZZ run1 = shfl_down_xyzz(run, 1);
+    if (active && g == 0) {
+#pragma unroll 1
+      for (int i = 0; i < 6; ++i) run1 = run1.dbl();
+      acc.add(acc1);
+      acc.add(run1);
+      store_xyzz(a.win + (((size_t)coset * a.lines + l) * nchunks + b) * MSM_WINDOWS + w, acc);
+    }
+  }
+}
+
+// sum_w 2^{8w} win[w] for each (coset, line, chunk)
+__global__ void k_msm_combine(const XYZZ* __restrict__ win, XYZZ* __restrict__ out, uint32_t count) {
+  uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= count) return;
+  const XYZZ* w = win + (size_t)i * MSM_WINDOWS;
+  XYZZ acc = load_xyzz(w + MSM_WINDOWS - 1);
+  for (int k = MSM_WINDOWS - 2; k >= 0; --k) {
+#pragma unroll 1
+    for (int d = 0; d < 8; ++d) acc = acc.dbl();
+    acc.add(load_xyzz(w + k));
+  }
+  store_xyzz(out + i, acc);
+}
+
+// ---------------------------------------------------------------------------
+// AMT aggregation (prove.rs:20-52 build_commitment_tree, prove_gpu.rs:89-123
+// aggregate_line / high commitment). part[c][l][b] are the per-chunk MSMs.
+// One CTA per (line, coset). Output nodes per coset, XYZZ, in the order
+//   [root][commitments[0] (2) .. commitments[LR-1] (R)][proofs[0] .. proofs[LR-1]][high]
+__device__ __forceinline__ uint32_t amt_commit_off(int d) { return 1 + ((2u << d) - 2); }
+__device__ __forceinline__ uint32_t amt_proof_off(int d, int lr) { return (2u << lr) - 1 + ((2u << d) - 2); }
+
+__global__ void k_amt_tree(XYZZ* __restrict__ part, XYZZ* __restrict__ nodes, int lr, int lines) {
+  const int l = blockIdx.x, c = blockIdx.y;
+  const int R = 1 << lr;
+  const uint32_t per_coset = 4u * R - 2;
+  XYZZ* p = part + ((size_t)c * lines + l) * R;
+  XYZZ* o = nodes + (size_t)c * per_coset;
+  // levels to reduce: quotient layer d = l + 1 keeps 2^d nodes; basis keeps all
+  // levels; high keeps 1
+  int keep_log = (l < lr) ? (l + 1) : 0;
+  const bool is_basis = (l == lr);
+  if (is_basis) {
+    for (int i = threadIdx.x; i < R; i += blockDim.x) o[amt_commit_off(lr - 1) + i] = p[i];
+  }
+  int cur = R;
+  int lvl = lr;  // current array holds 2^lvl nodes
+  while (lvl > keep_log) {
+    int half = cur >> 1;
+    __syncthreads();
+    // read pairs then write, two phases to allow in-place reduction
+    for (int base = 0; base < half; base += blockDim.x) {
+      int i = base + threadIdx.x;
+      XYZZ s;
+      if (i < half) {
+        s = p[2 * i];
+        s.add(p[2 * i + 1]);
+      }
+      __syncthreads();
+      if (i < half) p[i] = s;
+      __syncthreads();
+    }
+    cur = half;
+    --lvl;
+    if (is_basis) {
+      if (lvl >= 1) {
+        for (int i = threadIdx.x; i < cur; i += blockDim.x) o[amt_commit_off(lvl - 1) + i] = p[i];
+      } else if (threadIdx.x == 0) {
+        o[0] = p[0];
+      }
+    }
+  }
+  __syncthreads();
+  if (l < lr) {
+    for (int i = threadIdx.x; i < cur; i += blockDim.x) o[amt_proof_off(l, lr) + i] = p[i];
+  } else if (l == lr + 1) {
+    if (threadIdx.x == 0) o[per_coset - 1] = p[0];
+  }
+}
+
+// XYZZ node -> 64-byte ark G1
+__global__ void k_serialize_nodes(const XYZZ* __restrict__ nodes, uint8_t* __restrict__ out, uint32_t count) {
+  uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= count) return;
+  uint8_t buf[64];
+  g1_serialize(nodes[i], buf);
+  uint4* d = reinterpret_cast<uint4*>(out + (size_t)i * 64);
+  const uint32_t* w = reinterpret_cast<const uint32_t*>(buf);
+  d[0] = make_uint4(w[0], w[1], w[2], w[3]);
+  d[1] = make_uint4(w[4], w[5], w[6], w[7]);
+  d[2] = make_uint4(w[8], w[9], w[10], w[11]);
+  d[3] = make_uint4(w[12], w[13], w[14], w[15]);
+}
+
+// ---------------------------------------------------------------------------
+// Merkle tree (merkle/blob.rs:15-34): leaves = keccak(8 x 32 B), parents =
+// keccak(left || right) until 3 coset roots remain.
+__global__ void k_merkle_leaves(const uint8_t* __restrict__ data, uint8_t* __restrict__ leaves, uint32_t count) {
+  uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= count) return;
+  const uint64_t* src = reinterpret_cast<const uint64_t*>(data + (size_t)i * 256);
+  uint64_t in[32];
+#pragma unroll
+  for (int k = 0; k < 16; ++k) {
+    ulonglong2 v = reinterpret_cast<const ulonglong2*>(src)[k];
+    in[2 * k] = v.x;
+    in[2 * k + 1] = v.y;
+  }
+  uint64_t out[4];
+  keccak256_256(in, out);
+  ulonglong2* d = reinterpret_cast<ulonglong2*>(leaves + (size_t)i * 32);
+  d[0] = make_ulonglong2(out[0], out[1]);
+  d[1] = make_ulonglong2(out[2], out[3]);
+}
+__global__ void k_merkle_parents(const uint8_t* __restrict__ child, uint8_t* __restrict__ parent, uint32_t count) {
+  uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= count) return;
+  const ulonglong2* src = reinterpret_cast<const ulonglong2*>(child + (size_t)i * 64);
+  uint64_t in[8];
+#pragma unroll
+  for (int k = 0; k < 4; ++k) {
+    ulonglong2 v = src[k];
+    in[2 * k] = v.x;
+    in[2 * k + 1] = v.y;
+  }
+  uint64_t out[4];
+  keccak256_64(in, out);
+  ulonglong2* d = reinterpret_cast<ulonglong2*>(parent + (size_t)i * 32);
+  d[0] = make_ulonglong2(out[0], out[1]);
+  d[1] = make_ulonglong2(out[2], out[3]);
+}
+// keccak(keccak(r0 || r1) || r2)  (encoder/blob.rs:64-72)
+__global__ void k_file_root(const uint8_t* __restrict__ roots, uint8_t* __restrict__ out) {
+  if (threadIdx.x != 0 || blockIdx.x != 0) return;
+  const uint64_t* r = reinterpret_cast<const uint64_t*>(roots);
+  uint64_t in[8], t[4];
+  for (int k = 0; k < 8; ++k) in[k] = r[k];
+  keccak256_64(in, t);
+  for (int k = 0; k < 4; ++k) { in[k] = t[k]; in[4 + k] = r[8 + k]; }
+  keccak256_64(in, t);
+  uint64_t* o = reinterpret_cast<uint64_t*>(out);
+  for (int k = 0; k < 4; ++k) o[k] = t[k];
+}
+
+// ---------------------------------------------------------------------------
+// EncodedSlice serialisation (ark-serialize 0.4 derive, uncompressed):
+//   index | amt{index | commitment | row{index | len,row | len,proof | high}}
+//   | merkle{roots[3] | len,proof | leaf_index | leaf}
+// (encoder/slice.rs:15-20, amt/slice.rs:13-18, blob/encode.rs:202-209,
+//  proofs.rs:34-35, merkle/slice.rs:12-19). One CTA per slice.
+struct SliceArgs {
+  const uint8_t* enc;    // [3][R][C] x 32
+  const uint8_t* amt;    // [3][4R-2] x 64
+  const uint8_t* tree;   // Merkle levels, level d at tree_off[d]
+  const uint64_t* tree_off;
+  uint8_t* out;          // [3R][slice_size]
+  int lr, lc;
+  uint64_t slice_size;
+};
+__device__ __forceinline__ void put_u64(uint8_t* p, uint64_t v) {
+#pragma unroll
+  for (int i = 0; i < 8; ++i) p[i] = (uint8_t)(v >> (8 * i));
+}
+__global__ void k_slices(SliceArgs a) {
+  const int R = 1 << a.lr, C = 1 << a.lc;
+  const uint32_t index = blockIdx.x;
+  const uint32_t coset = index / R, local = index % R;
+  uint8_t* o = a.out + (uint64_t)index * a.slice_size;
+  const uint8_t* amt = a.amt + (size_t)coset * (4 * R - 2) * 64;
+  // row data, 16-byte vectors (offset 96 is 16-byte aligned when slice_size is)
+  const uint4* row = reinterpret_cast<const uint4*>(a.enc + ((size_t)coset * R + local) * C * 32);
+  uint8_t* rowdst = o + 96;
+  for (int k = threadIdx.x; k < C * 2; k += blockDim.x) {
+    uint4 v = row[k];
+    uint8_t* d = rowdst + 16 * k;
+    const uint8_t* s = reinterpret_cast<const uint8_t*>(&v);
+#pragma unroll
+    for (int i = 0; i < 16; ++i) d[i] = s[i];
+  }
+  const uint32_t rev = brev_bits(local, a.lr);
+  uint8_t* after = o + 96 + (size_t)32 * C;
+  // proof pairs: 8 + 128 LR bytes
+  if (threadIdx.x == 0) {
+    put_u64(o, index);
+    put_u64(o + 8, index);
+    put_u64(o + 80, local);
+    put_u64(o + 88, (uint64_t)C);
+    put_u64(after, (uint64_t)a.lr);
+  }
+  for (int k = threadIdx.x; k < 64; k += blockDim.x) o[16 + k] = amt[k];  // commitment (root)
+  for (int e = threadIdx.x; e < a.lr * 128; e += blockDim.x) {
+    int dd = e / 128, off = e % 128;
+    uint32_t lv = rev >> (a.lr - 1 - dd);
+    uint32_t node = lv ^ 1;
+    const uint8_t* src = (off < 64) ? amt + (size_t)(1 + (2u << dd) - 2 + node) * 64 + off
+                                    : amt + (size_t)((2u << a.lr) - 1 + (2u << dd) - 2 + node) * 64 + (off - 64);
+    after[8 + e] = *src;
+  }
+  uint8_t* high = after + 8 + 128 * a.lr;
+  for (int k = threadIdx.x; k < 64; k += blockDim.x) high[k] = amt[(size_t)(4 * R - 3) * 64 + k];
+  uint8_t* mk = high + 64;
+  const uint8_t* roots = a.tree + a.tree_off[0];
+  for (int k = threadIdx.x; k < 96; k += blockDim.x) mk[k] = roots[k];
+  if (threadIdx.x == 0) put_u64(mk + 96, (uint64_t)a.lr);
+  for (int e = threadIdx.x; e < a.lr * 32; e += blockDim.x) {
+    int i = e / 32, off = e % 32;
+    int d = a.lr - i;  // d = LR .. 1
+    uint32_t idx = index >> (a.lr - d);
+    mk[104 + e] = a.tree[a.tree_off[d] + (size_t)(idx ^ 1) * 32 + off];
+  }
+  uint8_t* tail = mk + 104 + 32 * a.lr;
+  if (threadIdx.x == 0) put_u64(tail, index);
+  for (int k = threadIdx.x; k < 32; k += blockDim.x) tail[8 + k] = a.tree[a.tree_off[a.lr] + (size_t)index * 32 + k];
+}
+
+// ---------------------------------------------------------------------------
+// parameter building (seeded tau; scalar domain then fixed-base multiply)
+
+// out[i] = x^i (Montgomery) for i < n
+__global__ void k_powers(Fr x, Fr* out, uint32_t n) {
+  uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  out[i] = x.pow_u64(i);
+}
+__global__ void k_scale(Fr* v, Fr s, uint32_t n) {
+  uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < n) v[i] = v[i] * s;
+}
+// quotient coefficient vector of layer d: c[i] = pw[M - i] for 1 <= i <= M, else 0
+__global__ void k_quot_coeff(const Fr* pw, Fr* c, uint32_t M, uint32_t n) {
+  uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  c[i] = (i >= 1 && i <= M) ? pw[M - i] : Fr::zero();
+}
+
+// generic four-step NTT pass A: for each column s (C of them) of x viewed as
+// [R][C] row-major: R-point transform over q, times w_N^{s r}; writes Y[r][s].
+__global__ void k_ntt4_colpass(const Fr* __restrict__ x, Fr* __restrict__ y, int lr, int lc,
+                               const Fr* __restrict__ tw_r, const Fr* __restrict__ w_lo,
+                               const Fr* __restrict__ w_hi) {
+  extern __shared__ __align__(16) uint8_t smem[];
+  const int R = 1 << lr, C = 1 << lc;
+  Fr* s = reinterpret_cast<Fr*>(smem);
+  const uint32_t col = blockIdx.x;
+  for (int q = threadIdx.x; q < R; q += blockDim.x) s[brev_bits(q, lr)] = load_fr(x + (size_t)q * C + col);
+  __syncthreads();
+  ntt_smem(s, lr, tw_r);
+  const uint32_t nmask = (1u << (lr + lc)) - 1;
+  for (int r = threadIdx.x; r < R; r += blockDim.x)
+    store_fr(y + (size_t)r * C + col, s[r] * pow_split(w_lo, w_hi, col * (uint32_t)r, lc, nmask));
+}
+// pass B: for each r, C-point transform over s of Y[r][*]; out[j R + r]
+__global__ void k_ntt4_rowpass(const Fr* __restrict__ y, Fr* __restrict__ out, int lr, int lc,
+                               const Fr* __restrict__ tw_c) {
+  extern __shared__ __align__(16) uint8_t smem[];
+  const int R = 1 << lr, C = 1 << lc;
+  Fr* s = reinterpret_cast<Fr*>(smem);
+  const uint32_t r = blockIdx.x;
+  for (int k = threadIdx.x; k < C; k += blockDim.x) s[brev_bits(k, lc)] = load_fr(y + (size_t)r * C + k);
+  __syncthreads();
+  ntt_smem(s, lc, tw_c);
+  for (int j = threadIdx.x; j < C; j += blockDim.x) store_fr(out + (size_t)j * R + r, s[j]);
+}
+
+// fixed-base table of G: tab[w*255 + d - 1] = d * 2^{8w} * G (XYZZ)
+__global__ void k_fixed_table(XYZZ* tab, G1Aff g) {
+  int w = blockIdx.x * blockDim.x + threadIdx.x;
+  if (w >= 32) return;
+  XYZZ base = XYZZ::from_affine(g);
+  for (int i = 0; i < 8 * w; ++i) base = base.dbl();
+  XYZZ acc = base;
+  for (int d = 1; d <= 255; ++d) {
+    tab[w * 255 + d - 1] = acc;
+    acc.add(base);
+  }
+}
+__global__ void k_xyzz_to_affine(const XYZZ* in, G1Aff* out, uint32_t n) {
+  uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  G1Aff a;
+  if (!in[i].to_affine(a)) { a.x = Fq::zero(); a.y = Fq::zero(); }
+  out[i] = a;
+}
+// out[p] = s[bitrev(p)] * G (enact: normalize + index_reverse, generate.rs:122-126)
+__global__ void k_fixed_mul(const G1Aff* __restrict__ tab, const Fr* __restrict__ sc, G1Aff* __restrict__ out,
+                            uint32_t n, int logn) {
+  uint32_t p = blockIdx.x * blockDim.x + threadIdx.x;
+  if (p >= n) return;
+  Fr s = sc[brev_bits(p, logn)].to_canonical();
+  XYZZ acc = XYZZ::inf();
+#pragma unroll 1
+  for (int w = 0; w < 32; ++w) {
+    uint32_t d = (s.v[w >> 2] >> (8 * (w & 3))) & 0xff;
+    if (d) {
+      G1Aff t = tab[w * 255 + d - 1];
+      acc.add_affine(t.x, t.y);
+    }
+  }
+  G1Aff a;
+  if (!acc.to_affine(a)) { a.x = Fq::zero(); a.y = Fq::zero(); }
+  out[p] = a;
+}
+
+}  // namespace zg

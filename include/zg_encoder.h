@@ -1,0 +1,122 @@
+/*
+ * zg_encoder.h — C ABI of the B200 blob encoder for the 0G DA encoder path.
+ *
+ * The reference (0glabs/0g-da-encoder, Rust) exposes this path as
+ *   - the gRPC service Encoder.EncodeBlob            grpc/proto/encoder.proto:5-21
+ *   - EncoderService::process_data(&[u8], bool)        grpc/src/service.rs:67-105
+ *   - EncodedBlob::build / get_row / get_commitment /
+ *     get_roots / get_file_root / get_data             crates/encoder/src/encoder/blob.rs:32-62
+ *   - RawData::try_from(&[u8]) -> TooLargeBlob         crates/encoder/src/raw_data.rs:76-95
+ *   - ZgEncoderParams::from_dir_mont(dir, .., None)    crates/amt/src/blob/encode.rs:114-132
+ *   - AMTProofs::gen_amt_proofs (plugin point)         crates/amt/src/prove_params/interfaces.rs:7-15
+ * Every entry point below names the reference item it replaces. Plain
+ * pointers and sizes only; no exceptions or panics cross this boundary.
+ *
+ * Status codes: ZG_OK (0); ZG_ERR_TOO_LARGE_BLOB (1) is the reference's only
+ * recoverable encoder error (EncoderError::TooLargeBlob); negative values are
+ * configuration / device errors. zg_last_error() returns the message of the
+ * calling thread's last failure; for ZG_ERR_TOO_LARGE_BLOB it is the
+ * reference's Debug text "TooLargeBlob { actual: A, expected_max: M }" that
+ * the gRPC layer returns as Status::Unknown (grpc/src/service.rs:61).
+ */
+#ifndef ZG_ENCODER_H
+#define ZG_ENCODER_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define ZG_OK 0
+#define ZG_ERR_TOO_LARGE_BLOB 1
+#define ZG_ERR_INVALID_ARG (-1)
+#define ZG_ERR_CUDA (-2)
+#define ZG_ERR_PARAMS (-3)
+#define ZG_ERR_INTERNAL (-4)
+
+typedef struct zg_ctx zg_ctx;
+typedef struct zg_reply zg_reply;
+
+typedef struct zg_config {
+  uint32_t log_row;        /* BLOB_ROW_LOG (crates/encoder/src/constants.rs:14), 10 in production */
+  uint32_t log_col;        /* BLOB_COL_LOG (constants.rs:15), 10 in production */
+  uint64_t tau_seed;       /* params from a seeded tau when params_dir is NULL */
+  const char* params_dir;  /* else: amt-prove-coset{0,1,2}-mont-*-{LR:02}-{LR+LC:02}.bin */
+  int device;              /* CUDA device ordinal */
+} zg_config;
+
+/* Builds the device-resident encoder params (3 cosets x (LR + 2) G1 lines).
+ * Replaces ZgEncoderParams::from_dir_mont (crates/amt/src/blob/encode.rs:114-132)
+ * and, for the seeded case, PowerTau::setup_inner + AMTParams::from_pp
+ * (crates/amt/src/power_tau.rs:54-80, prove_params/generate.rs:139-263). */
+int zg_ctx_create(const zg_config* cfg, zg_ctx** out);
+void zg_ctx_destroy(zg_ctx* ctx);
+/* ZgEncoderParams::warmup (crates/amt/src/blob/encode.rs:85-89): runs one
+ * encode of an empty payload so later calls see warm caches. */
+int zg_ctx_warmup(zg_ctx* ctx);
+
+/* EncoderService::process_data (grpc/src/service.rs:67-105): payload bytes ->
+ * EncodeBlobReply. `data` is host memory. On ZG_OK *out owns the reply. */
+int zg_encode(zg_ctx* ctx, const uint8_t* data, size_t len, int require_data, zg_reply** out);
+void zg_reply_free(zg_reply* r);
+uint32_t zg_reply_version(const zg_reply* r);                              /* service.rs:98 */
+const uint8_t* zg_reply_erasure_commitment(const zg_reply* r, size_t* len); /* service.rs:77-83, 64 B */
+const uint8_t* zg_reply_storage_root(const zg_reply* r, size_t* len);       /* get_file_root, 32 B */
+const uint8_t* zg_reply_encoded_data(const zg_reply* r, size_t* len);       /* get_data, service.rs:85-91 */
+size_t zg_reply_num_slices(const zg_reply* r);                              /* BLOB_ROW_ENCODED */
+const uint8_t* zg_reply_slice(const zg_reply* r, size_t index, size_t* len);/* get_row(i) serialized */
+const uint8_t* zg_reply_roots(const zg_reply* r, size_t* len);              /* EncodedBlob::get_roots, 96 B */
+
+/* Device-resident variant of zg_encode: `d_data` is device memory, results
+ * stay in context-owned device buffers (valid until the next encode on the
+ * same context) and the call returns after queuing work on `stream`
+ * (cudaStream_t, NULL = the context stream). Same math as zg_encode. */
+typedef struct zg_device_blob {
+  const uint8_t* encoded_data;  /* [3][R][C] x 32 B, canonical */
+  const uint8_t* slices;        /* [3R] x slice_size, serialized EncodedSlice */
+  size_t slice_size;
+  const uint8_t* amt_outputs;   /* [3][4R-2] x 64 B ark G1: root, commitment tree, proof layers, high */
+  const uint8_t* roots;         /* 3 x 32 B */
+  const uint8_t* file_root;     /* 32 B */
+} zg_device_blob;
+int zg_encode_device(zg_ctx* ctx, const void* d_data, size_t len, void* stream, zg_device_blob* out);
+
+/* Copy of one device param line (N points, 64 B mont x||y each), the layout
+ * of the reference's mont files (fast_serde_bn254.rs:139-160). line < LR:
+ * quotients[line]; LR: basis; LR+1: high_basis. */
+int zg_ctx_param_line(zg_ctx* ctx, int coset, int line, uint8_t* host_out, size_t cap);
+
+/* Kernel-level entry points (device pointers, stream-ordered on `stream`).
+ * zg_msm_chunks: the AMT plugin's MSM decomposition (prove_gpu.rs:55-87):
+ * for every line l < lines and chunk b < nchunks,
+ *   out[l][b] = sum_t scalars[b*chunk + t] * bases[l][b*chunk + t]
+ * written as 64-byte ark G1. scalars: canonical 32 B; bases: mont x||y.
+ * nchunks and chunk are powers of two, chunk <= 1024. */
+int zg_msm_chunks(const void* d_bases, const void* d_scalars, uint32_t lines, uint32_t log_nchunks,
+                  uint32_t log_chunk, void* d_out, void* stream);
+/* Batched radix-2 NTT over Fr with ark-poly Radix2EvaluationDomain semantics
+ * (crates/amt/src/blob/encode.rs:142-157): `batch` contiguous vectors of
+ * 2^log_n canonical 32-byte elements, transformed in place. inverse != 0
+ * applies the 1/n scaled inverse. coset_idx > 0 (forward only) multiplies
+ * coefficient i by coset_factor(2^log_n, coset_idx)^i first (to_coset_blob). */
+int zg_ntt(void* d_data, uint32_t log_n, uint32_t batch, int inverse, uint32_t coset_idx, void* stream);
+/* Keccak-256 Merkle levels (crates/encoder/src/merkle/blob.rs:15-34) over
+ * n_items 32-byte items: leaves = keccak(8 items), then pairwise parents
+ * until <= 3 nodes; writes the 3 roots (or fewer) to d_roots. */
+int zg_merkle_roots(const void* d_items, size_t n_items, void* d_roots, void* stream);
+
+/* Device arithmetic self test (no reference counterpart): compares the device
+ * field and curve routines against the host build of the same code on fixed
+ * pseudo-random inputs; fails[k] receives the mismatch count of check k
+ * (0 Fq mul, 1 Fq mul with immediate modulus, 2 Fq add, 3 Fq sub, 4 Fr mul,
+ * 5 Fr Montgomery round trip, 6 XYZZ add(P, P) == dbl(P)). */
+int zg_selftest(int* fails, int nops);
+
+const char* zg_last_error(void);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* ZG_ENCODER_H */

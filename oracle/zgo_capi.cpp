@@ -222,6 +222,63 @@ int zgo_param_points(int log_row, int log_col, uint64_t seed, int coset, int lin
   return 0;
 }
 
+
+// Merkle roots (merkle/blob.rs:15-34) of n_items 32-byte items; writes 3 x 32 B
+void zgo_merkle_roots(int log_row, int log_col, const uint8_t* items, uint8_t out[96]) {
+  Dims d = {log_row, log_col};
+  std::vector<H256> data(COSET_N * d.n());
+  for (size_t i = 0; i < data.size(); ++i) memcpy(data[i].data(), items + 32 * i, 32);
+  Merkle m = merkle_build(d, std::move(data));
+  for (int c = 0; c < COSET_N; ++c) memcpy(out + 32 * c, m.tree[0][c].data(), 32);
+}
+
+// Verifier params (AMTVerifyParams: basis, vanishes, g2, high_g2;
+// crates/amt/src/verify_params.rs:22-28) with the basis lines supplied by the
+// caller (3 x N points, 64 B mont each) and the G2 parts from the scalar
+// domain of the seeded tau.
+void* zgo_verify_params_new(int log_row, int log_col, uint64_t seed, const uint8_t* basis_lines) {
+  auto* h = new ParamsHandle();
+  h->d = {log_row, log_col};
+  h->tau = tau_from_seed(seed);
+  h->has_tau = true;
+  int depth = log_row + log_col;
+  size_t n = h->d.n();
+  for (int c = 0; c < COSET_N; ++c) {
+    AMTScalars s;
+    {
+      // only the G2 part of the scalar-domain builder is needed
+      size_t length = n;
+      size_t high_start = (size_t(1) << (depth + 2)) - length;
+      Fr w = c > 0 ? coset_factor(length, c).inverse() : Fr::one();
+      Fr tp = h->tau * w;
+      std::vector<Fr> pw(length);
+      pw[0] = Fr::one();
+      for (size_t i = 1; i < length; ++i) pw[i] = pw[i - 1] * tp;
+      for (int dd = 1; dd <= log_row; ++dd) {
+        size_t step = size_t(1) << (depth - dd);
+        size_t sz = size_t(1) << dd;
+        std::vector<Fr> coeff(sz, Fr::zero());
+        coeff[0] = pw[length - step];
+        for (size_t i = 1; i < length / step; ++i) coeff[i] = pw[(i - 1) * step];
+        fr_ntt_omega(coeff, fr_root_of_unity(dd).inverse());
+        index_reverse(coeff);
+        s.vanishes.push_back(coeff);
+      }
+      s.high_g2 = h->tau.pow_u64(high_start);
+    }
+    AMTParams p = amt_from_scalars(s, depth, log_row);
+    p.basis.resize(n);
+    for (size_t i = 0; i < n; ++i) {
+      u64 x[4], y[4];
+      memcpy(x, basis_lines + (c * n + i) * 64, 32);
+      memcpy(y, basis_lines + (c * n + i) * 64 + 32, 32);
+      p.basis[i] = {Fq::from_raw_mont(x), Fq::from_raw_mont(y), false};
+    }
+    h->amt[c] = p;
+  }
+  return h;
+}
+
 // ---- encode -------------------------------------------------------------------
 // returns nullptr and *err = 1 for TooLargeBlob
 void* zgo_encode(void* params, const uint8_t* data, size_t len, int* err) {

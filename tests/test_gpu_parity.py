@@ -1,0 +1,309 @@
+"""GPU parity: the CUDA path, called through the C ABI, against the CPU oracle.
+
+Integer / field / byte work: every comparison is bit-exact.
+"""
+import ctypes
+import random
+
+import numpy as np
+import pytest
+
+import zgo
+
+pytestmark = pytest.mark.gpu
+
+R_MOD = zgo.R_MOD
+Q_MOD = zgo.Q_MOD
+
+
+def torch_mod():
+    import torch
+    return torch
+
+
+def rand_fr_bytes(rng, n):
+    """n canonical Fr elements, 32 B little-endian each (top byte < 0x30)."""
+    b = rng.integers(0, 256, size=(n, 32), dtype=np.uint8)
+    b[:, 31] = rng.integers(0, 0x30, size=n, dtype=np.uint8)
+    return b.tobytes()
+
+
+def dev(buf: bytes):
+    torch = torch_mod()
+    t = torch.frombuffer(bytearray(buf), dtype=torch.uint8).cuda()
+    return t
+
+
+def host(t) -> bytes:
+    torch = torch_mod()
+    torch.cuda.synchronize()
+    return t.cpu().numpy().tobytes()
+
+
+def empty(n):
+    torch = torch_mod()
+    return torch.empty(n, dtype=torch.uint8, device="cuda")
+
+
+def mont_lines(mont: bytes, log_row, log_col):
+    """Split a mont params file into its G1 lines (fast_serde_bn254.rs:20-53)."""
+    n = 1 << (log_row + log_col)
+    off = 6 + 256
+    basis = mont[off:off + 64 * n]
+    off += 64 * n
+    quot = []
+    for _ in range(log_row):
+        quot.append(mont[off:off + 64 * n])
+        off += 64 * n
+    for d in range(log_row):
+        off += 128 * (2 << d)
+    high = mont[off:off + 64 * n]
+    return quot + [basis, high]
+
+
+# ---------------------------------------------------------------------------
+@pytest.mark.parametrize("log_n,batch,inverse,coset", [
+    (5, 4, 0, 0), (5, 4, 1, 0), (5, 3, 0, 1), (10, 8, 0, 0), (10, 8, 1, 0), (10, 2, 0, 2),
+    (11, 2, 1, 0), (14, 1, 0, 0), (14, 1, 1, 0), (20, 1, 0, 1), (20, 1, 1, 0),
+])
+def test_ntt_matches_oracle(gpu_pkg, oracle, log_n, batch, inverse, coset):
+    rng = np.random.default_rng(log_n * 100 + batch + inverse)
+    n = 1 << log_n
+    data = rand_fr_bytes(rng, n * batch)
+    t = dev(data)
+    rc = gpu_pkg.lib().zg_ntt(t.data_ptr(), log_n, batch, inverse, coset, None)
+    assert rc == 0, gpu_pkg.lib().zg_last_error()
+    got = host(t)
+    for b in range(batch):
+        vec = data[b * n * 32:(b + 1) * n * 32]
+        exp = oracle.ntt(vec, inverse=bool(inverse), coset_idx=coset, coset_len=n)
+        assert got[b * n * 32:(b + 1) * n * 32] == exp, f"vector {b}"
+
+
+def _neg_mont_point(p: bytes) -> bytes:
+    y = int.from_bytes(p[32:], "little")
+    return p[:32] + ((Q_MOD - y) % Q_MOD).to_bytes(32, "little")
+
+
+@pytest.fixture(scope="module")
+def small_params_mont(oracle):
+    op = oracle.params(4, 6, 7)
+    return [op.mont(c) for c in range(3)]
+
+
+def test_msm_chunks_matches_oracle(gpu_pkg, oracle, small_params_mont):
+    lines = mont_lines(small_params_mont[0], 4, 6)
+    rng = np.random.default_rng(5)
+    n = 1 << 10
+    bases = b"".join(lines[:3])  # 3 lines of 1024 points
+    scal = bytearray(rand_fr_bytes(rng, n))
+    # edge scalars: zero, one, r - 1, small
+    for i, v in enumerate([0, 1, R_MOD - 1, 2, 255, 256, 1 << 253]):
+        scal[32 * i:32 * i + 32] = v.to_bytes(32, "little")
+    scal = bytes(scal)
+    out = empty(3 * 16 * 64)
+    tb, ts = dev(bases), dev(scal)  # keep the device buffers alive across the call
+    rc = gpu_pkg.lib().zg_msm_chunks(tb.data_ptr(), ts.data_ptr(), 3, 4, 6, out.data_ptr(), None)
+    assert rc == 0, gpu_pkg.lib().zg_last_error()
+    got = host(out)
+    for l in range(3):
+        for b in range(16):
+            exp = oracle.msm(lines[l][64 * 64 * b:64 * 64 * (b + 1)], scal[32 * 64 * b:32 * 64 * (b + 1)])
+            assert got[(l * 16 + b) * 64:(l * 16 + b + 1) * 64] == exp, (l, b)
+
+
+def test_msm_special_cases(gpu_pkg, oracle, small_params_mont):
+    """Doubling and cancellation inside buckets: repeated and negated bases."""
+    line = mont_lines(small_params_mont[0], 4, 6)[0]
+    pts = [line[64 * i:64 * i + 64] for i in range(8)]
+    chunk = []
+    for i in range(32):
+        p = pts[i % 4]
+        chunk.append(_neg_mont_point(p) if (i // 4) % 2 else p)
+    bases = b"".join(chunk)
+    scal = b"".join(((i % 3) + 5).to_bytes(32, "little") for i in range(32))
+    zero = bytes(32 * 32)
+    out = empty(2 * 64)
+    b2 = bases + bases
+    s2 = scal + zero
+    tb, ts = dev(b2), dev(s2)
+    rc = gpu_pkg.lib().zg_msm_chunks(tb.data_ptr(), ts.data_ptr(), 1, 1, 5, out.data_ptr(), None)
+    assert rc == 0
+    got = host(out)
+    assert got[:64] == oracle.msm(bases, scal)
+    assert got[64:] == oracle.msm(bases, zero)
+    assert got[127] == 0x40  # zero scalars give the point at infinity
+
+
+@pytest.mark.parametrize("log_row,log_col", [(4, 6), (6, 5), (3, 5)])
+def test_params_match_oracle(gpu_pkg, oracle, log_row, log_col):
+    seed = 1234 + log_row
+    params = gpu_pkg.ZgEncoderParams.from_seed(log_row, log_col, seed)
+    op = oracle.params(log_row, log_col, seed)
+    for c in range(3):
+        lines = mont_lines(op.mont(c), log_row, log_col)
+        for l, exp in enumerate(lines):
+            assert params.param_line(c, l) == exp, (c, l)
+    params.close()
+
+
+def _check_against_oracle(pkg, oracle, params, op, payload, verify_all=False):
+    reply = pkg.EncoderService(params).process_data(payload, True)
+    ob = oracle.encode(op, payload)
+    assert reply.version == 0
+    assert reply.erasure_commitment == ob.commitment()
+    assert reply.storage_root == ob.file_root()
+    assert reply.encoded_data == ob.data()
+    d = params.dims
+    assert len(reply.encoded_slice) == d.rows_encoded
+    for i, s in enumerate(reply.encoded_slice):
+        assert len(s) == d.slice_size
+        assert s == ob.slice(i), f"slice {i}"
+    if verify_all:
+        for i, s in enumerate(reply.encoded_slice):
+            rc, det = oracle.verify(op, s, reply.erasure_commitment, reply.storage_root)
+            assert rc == zgo.V_OK, (i, rc, det)
+    return reply
+
+
+@pytest.mark.parametrize("log_row,log_col", [(4, 6), (6, 5)])
+def test_encode_matches_oracle(gpu_pkg, oracle, log_row, log_col):
+    """EncodedBlob::build parity for payload sizes 0, 1, 1234, MAX and MAX+1
+    (the cases of test_batcher_and_verify, crates/encoder/src/encoder/blob.rs:282-293)."""
+    seed = 99
+    params = gpu_pkg.ZgEncoderParams.from_seed(log_row, log_col, seed)
+    op = oracle.params(log_row, log_col, seed)
+    d = params.dims
+    rng = np.random.default_rng(222)
+    for n in (0, 1, 1234, d.max_raw_data_size):
+        payload = rng.integers(0, 256, size=n, dtype=np.uint8).tobytes()
+        _check_against_oracle(gpu_pkg, oracle, params, op, payload, verify_all=(n == 1234))
+    with pytest.raises(gpu_pkg.TooLargeBlob) as ei:
+        gpu_pkg.EncoderService(params).process_data(bytes(d.max_raw_data_size + 1), False)
+    assert ei.value.actual == d.max_raw_data_size + 1
+    assert ei.value.expected_max == d.max_raw_data_size
+    params.close()
+
+
+def test_encode_zero_blob_is_infinity(gpu_pkg, oracle):
+    """An empty payload encodes to the all-zero blob: every commitment and
+    proof is the point at infinity (ark flag bit 6)."""
+    params = gpu_pkg.ZgEncoderParams.from_seed(4, 6, 5)
+    reply = gpu_pkg.EncoderService(params).process_data(b"", False)
+    assert reply.erasure_commitment == bytes(64)
+    assert reply.encoded_data == b""
+    s = reply.encoded_slice[0]
+    assert s[16:80] == bytes(63) + b"\x40"
+    params.close()
+
+
+def test_merkle_roots_match_oracle(gpu_pkg, oracle):
+    rng = np.random.default_rng(3)
+    log_row, log_col = 5, 6
+    n = 3 << (log_row + log_col)
+    items = rng.integers(0, 256, size=32 * n, dtype=np.uint8).tobytes()
+    out = empty(96)
+    ti = dev(items)
+    rc = gpu_pkg.lib().zg_merkle_roots(ti.data_ptr(), n, out.data_ptr(), None)
+    assert rc == 0
+    assert host(out) == oracle.merkle_roots(log_row, log_col, items)
+
+
+# ---------------------------------------------------------------------------
+# production shape: 1024 x 1024, full payload
+@pytest.fixture(scope="module")
+def prod(gpu_pkg):
+    seed = 2024
+    params = gpu_pkg.ZgEncoderParams.from_seed(10, 10, seed)
+    rng = np.random.default_rng(222)
+    payload = rng.integers(0, 256, size=params.dims.max_raw_data_size, dtype=np.uint8).tobytes()
+    reply = gpu_pkg.EncoderService(params).process_data(payload, True)
+    yield params, seed, payload, reply
+    params.close()
+
+
+def test_production_params_sample(prod, oracle):
+    params, seed, _, _ = prod
+    idx = [0, 1, 2, 777, 65535, 524288, 1048575]
+    for c in range(3):
+        for line in (0, 9, 10, 11):
+            got = params.param_line(c, line)
+            exp = oracle.param_points(10, 10, seed, c, line, idx)
+            for k, i in enumerate(idx):
+                assert got[64 * i:64 * i + 64] == exp[64 * k:64 * k + 64], (c, line, i)
+
+
+def test_production_encoded_data(prod, oracle):
+    params, seed, payload, reply = prod
+    d = params.dims
+    N = d.raw_blob_size
+    data = reply.encoded_data
+    assert len(data) == 3 * N * 32
+    # coset 0 is the raw blob: 31-byte chunks + a zero byte
+    raw = gpu_mod_raw(payload, d)
+    c0 = np.frombuffer(data[:N * 32], dtype=np.uint8).reshape(N, 32)
+    assert np.array_equal(c0[:, :31], np.frombuffer(raw, dtype=np.uint8).reshape(N, 31))
+    assert not c0[:, 31].any()
+    # cosets 1, 2: to_coset_blob of the column-major points (encode.rs:135-158)
+    pts = c0.reshape(d.rows, d.cols, 32).transpose(1, 0, 2).copy().tobytes()
+    coeff = oracle.ntt(pts, inverse=True)
+    for c in (1, 2):
+        ev = oracle.ntt(coeff, coset_idx=c, coset_len=N)
+        ev = np.frombuffer(ev, dtype=np.uint8).reshape(d.cols, d.rows, 32).transpose(1, 0, 2).copy().tobytes()
+        assert data[c * N * 32:(c + 1) * N * 32] == ev, f"coset {c}"
+
+
+def gpu_mod_raw(payload, d):
+    buf = bytearray(d.max_blob_size)
+    buf[:len(payload)] = payload
+    buf[d.max_raw_data_size:] = len(payload).to_bytes(4, "little")
+    return bytes(buf)
+
+
+def test_production_merkle(prod, oracle):
+    params, _, _, reply = prod
+    roots = oracle.merkle_roots(10, 10, reply.encoded_data)
+    s = reply.encoded_slice[0]
+    off = 96 + 32 * 1024 + 8 + 128 * 10 + 64
+    assert s[off:off + 96] == roots
+    assert reply.storage_root == oracle.keccak256(oracle.keccak256(roots[:64]) + roots[64:])
+
+
+def test_production_amt_scalar_domain(prod, oracle):
+    """Every AMT output (commitment tree, proof layers, high commitment) equals
+    (sum_t scalar_t * s_t) * G1 where s_t are the param scalars of the seeded tau."""
+    params, seed, _, reply = prod
+    N = params.dims.raw_blob_size
+    exp = [oracle.amt_scalar_domain(10, 10, seed, c, reply.encoded_data[c * N * 32:(c + 1) * N * 32])
+           for c in range(3)]
+    assert exp[0][:64] == exp[1][:64] == exp[2][:64]
+    com = exp[0][:64]
+    # reply commitment: x || y without flags
+    assert reply.erasure_commitment[:63] == com[:63]
+    assert reply.erasure_commitment[63] == com[63] & 0x3f
+    R = 1024
+    for c in range(3):
+        for local in (0, 1, 513, 1023):
+            s = reply.encoded_slice[c * R + local]
+            rev = int(format(local, "010b")[::-1], 2)
+            after = 96 + 32 * 1024
+            for dd in range(10):
+                lv = rev >> (10 - 1 - dd)
+                node = lv ^ 1
+                ci = 1 + (2 << dd) - 2 + node
+                pi = (2 * R - 1) + (2 << dd) - 2 + node
+                pair = s[after + 8 + 128 * dd: after + 8 + 128 * (dd + 1)]
+                assert pair[:64] == exp[c][64 * ci:64 * ci + 64], (c, local, dd)
+                assert pair[64:] == exp[c][64 * pi:64 * pi + 64], (c, local, dd)
+            high = s[after + 8 + 1280: after + 8 + 1280 + 64]
+            assert high == exp[c][64 * (4 * R - 3):64 * (4 * R - 2)]
+
+
+def test_production_slices_verify(prod, oracle):
+    params, seed, _, reply = prod
+    basis = b"".join(params.param_line(c, 10) for c in range(3))
+    vp = oracle.verify_params(10, 10, seed, basis)
+    rnd = random.Random(7)
+    for i in [0, 1023, 1024, 3071] + rnd.sample(range(3072), 4):
+        rc, det = oracle.verify(vp, reply.encoded_slice[i], reply.erasure_commitment, reply.storage_root)
+        assert rc == zgo.V_OK, (i, rc, det)
