@@ -45,6 +45,7 @@ class _Config(ctypes.Structure):
         ("tau_seed", ctypes.c_uint64),
         ("params_dir", ctypes.c_char_p),
         ("device", ctypes.c_int),
+        ("msm_window_bits", ctypes.c_uint32),
     ]
 
 
@@ -75,7 +76,11 @@ _SIGS = {
     "zg_reply_slice": (_P, [_P, _SZ, ctypes.POINTER(_SZ)]),
     "zg_reply_roots": (_P, [_P, ctypes.POINTER(_SZ)]),
     "zg_encode_device": (ctypes.c_int, [_P, _P, _SZ, _P, ctypes.POINTER(_DeviceBlob)]),
-    "zg_ctx_param_line": (ctypes.c_int, [_P, ctypes.c_int, ctypes.c_int, _P, _SZ]),
+    "zg_ctx_param_points": (ctypes.c_int, [_P, ctypes.c_int, ctypes.c_int, _SZ, _SZ, _P, _SZ]),
+    "zg_ctx_set_profiling": (ctypes.c_int, [_P, ctypes.c_int]),
+    "zg_ctx_phase_times": (ctypes.c_int, [_P, ctypes.POINTER(ctypes.c_float), ctypes.c_int]),
+    "zg_ctx_launches": (ctypes.c_uint64, [_P]),
+    "zg_probe_imad": (ctypes.c_int, [ctypes.c_int, ctypes.POINTER(ctypes.c_double)]),
     "zg_msm_chunks": (ctypes.c_int, [_P, _P, ctypes.c_uint32, ctypes.c_uint32, ctypes.c_uint32, _P, _P]),
     "zg_ntt": (ctypes.c_int, [_P, ctypes.c_uint32, ctypes.c_uint32, ctypes.c_int, ctypes.c_uint32, _P]),
     "zg_merkle_roots": (ctypes.c_int, [_P, _SZ, _P, _P]),
@@ -151,6 +156,13 @@ class Dims:
         return 312 + 32 * self.cols + 160 * self.log_row
 
 
+def probe_imad(device=0):
+    """Device integer multiply-add rate, 1e9/s."""
+    v = ctypes.c_double()
+    _check(lib().zg_probe_imad(device, ctypes.byref(v)))
+    return v.value
+
+
 def selftest():
     """Mismatch counts of the device arithmetic against its host build."""
     fails = (ctypes.c_int * 7)()
@@ -212,18 +224,18 @@ class ZgEncoderParams:
         self.dims = dims
 
     @classmethod
-    def from_seed(cls, log_row=10, log_col=10, seed=0, device=0):
+    def from_seed(cls, log_row=10, log_col=10, seed=0, device=0, msm_window_bits=0):
         """Params of a seeded tau, built on the GPU by the reference builder's
         rules (power_tau.rs:54-80, prove_params/generate.rs:139-263)."""
-        cfg = _Config(log_row, log_col, seed, None, device)
+        cfg = _Config(log_row, log_col, seed, None, device, msm_window_bits)
         h = ctypes.c_void_p()
         _check(lib().zg_ctx_create(ctypes.byref(cfg), ctypes.byref(h)))
         return cls(h, Dims(log_row, log_col))
 
     @classmethod
-    def from_dir_mont(cls, params_dir, log_row=10, log_col=10, device=0):
+    def from_dir_mont(cls, params_dir, log_row=10, log_col=10, device=0, msm_window_bits=0):
         """Params from the reference's mont files (amt-prove-coset{c}-mont-*.bin)."""
-        cfg = _Config(log_row, log_col, 0, os.fsencode(params_dir), device)
+        cfg = _Config(log_row, log_col, 0, os.fsencode(params_dir), device, msm_window_bits)
         h = ctypes.c_void_p()
         _check(lib().zg_ctx_create(ctypes.byref(cfg), ctypes.byref(h)))
         return cls(h, Dims(log_row, log_col))
@@ -235,11 +247,26 @@ class ZgEncoderParams:
     def warmup(self):
         _check(lib().zg_ctx_warmup(self._h))
 
-    def param_line(self, coset, line):
-        n = self.dims.raw_blob_size * 64
+    def param_line(self, coset, line, first=0, count=None):
+        """Points [first, first+count) of a param line, 64 B mont x||y each."""
+        if count is None:
+            count = self.dims.raw_blob_size - first
+        n = count * 64
         buf = ctypes.create_string_buffer(n)
-        _check(lib().zg_ctx_param_line(self._h, coset, line, buf, n))
+        _check(lib().zg_ctx_param_points(self._h, coset, line, first, count, buf, n))
         return buf.raw
+
+    def set_profiling(self, enable=True):
+        _check(lib().zg_ctx_set_profiling(self._h, 1 if enable else 0))
+
+    def phase_times(self):
+        """Last encode's phase durations (ms): rs, merkle, msm, aggregate, slices."""
+        ms = (ctypes.c_float * 5)()
+        _check(lib().zg_ctx_phase_times(self._h, ms, 5))
+        return dict(zip(["rs", "merkle", "msm", "aggregate", "slices"], list(ms)))
+
+    def launches(self):
+        return lib().zg_ctx_launches(self._h)
 
     def close(self):
         if self._h:

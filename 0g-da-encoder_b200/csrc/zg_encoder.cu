@@ -144,6 +144,11 @@ void free_twiddles(Twiddles* tw) {
   *tw = Twiddles();
 }
 
+size_t fb_sort_smem_bytes(int lc) {
+  size_t C = size_t(1) << lc;
+  return C * 32 + (FB_BUCKETS + 1) * 4 + 256 * 4 + (size_t)FB_WINDOWS * C * 2 + 16;
+}
+
 size_t msm_smem_bytes(int lc) {
   size_t C = size_t(1) << lc;
   return C * 32 + (size_t)MSM_WINDOWS * C * 2 + MSM_WINDOWS * 129 * 2 + 129 * 4 + 16;
@@ -159,6 +164,7 @@ int set_smem_limits() {
   ZG_CK(cudaFuncSetAttribute(k_cols, cudaFuncAttributeMaxDynamicSharedMemorySize, big));
   ZG_CK(cudaFuncSetAttribute(k_rows_ntt, cudaFuncAttributeMaxDynamicSharedMemorySize, big));
   ZG_CK(cudaFuncSetAttribute(k_msm_chunks, cudaFuncAttributeMaxDynamicSharedMemorySize, big));
+  ZG_CK(cudaFuncSetAttribute(k_fb_sort, cudaFuncAttributeMaxDynamicSharedMemorySize, big));
   ZG_CK(cudaFuncSetAttribute(k_ntt4_colpass, cudaFuncAttributeMaxDynamicSharedMemorySize, big));
   ZG_CK(cudaFuncSetAttribute(k_ntt4_rowpass, cudaFuncAttributeMaxDynamicSharedMemorySize, big));
   done = true;
@@ -187,7 +193,18 @@ struct zg_ctx {
   size_t max_blob = 0, max_raw = 0;
   cudaStream_t stream = nullptr;
   Twiddles tw;
-  G1Aff* bases = nullptr;  // [3][L][N]
+  // params with their fixed-base window multiples: tab[c][l][w][p] (W windows
+  // per line, window 0 = the param points themselves)
+  bool fb = false;
+  int W = 1;
+  G1Aff* tab = nullptr;
+  G1Aff* line_ptr(int c, int l) const { return tab + ((size_t)c * L + l) * W * N; }
+  uint32_t* fb_offs = nullptr;
+  uint16_t* fb_ents = nullptr;
+  XYZZ* fb_T = nullptr;
+  XYZZ* fb_S = nullptr;
+  XYZZ* fb_gbuf = nullptr;  // per persistent CTA bucket sums
+  unsigned fb_ctas = 0;
   uint8_t* raw = nullptr;
   uint8_t* enc = nullptr;
   Fr* T1 = nullptr;
@@ -205,6 +222,13 @@ struct zg_ctx {
   size_t slice_size = 0;
   uint8_t* file_root = nullptr;
   uint8_t* h_in = nullptr;  // pinned staging for payloads
+  // measurement: optional per-phase events and a count of kernel launches
+  bool profiling = false;
+  cudaEvent_t ev[6] = {nullptr, nullptr, nullptr, nullptr, nullptr, nullptr};
+  // completion of the last encode; every encode's stream waits on it first, so
+  // encodes issued on different streams never overlap on the shared scratch
+  cudaEvent_t done = nullptr;
+  uint64_t launches = 0;
   std::mutex mu;
 };
 
@@ -223,11 +247,22 @@ namespace {
 
 int alloc_blob_buffers(zg_ctx* c) {
   const size_t N = c->N, R = c->R;
+  if (c->fb) {
+    ZG_CK(cudaMalloc(&c->fb_offs, 3 * R * (FB_BUCKETS + 1) * sizeof(uint32_t)));
+    ZG_CK(cudaMalloc(&c->fb_ents, 3 * R * FB_WINDOWS * c->C * sizeof(uint16_t)));
+    ZG_CK(cudaMalloc(&c->fb_T, 3 * R * (size_t)c->L * FB_ACC_THREADS * sizeof(XYZZ)));
+    ZG_CK(cudaMalloc(&c->fb_S, 3 * R * (size_t)c->L * FB_ACC_THREADS * sizeof(XYZZ)));
+    int sms = 0, per_sm = 0;
+    ZG_CK(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, c->device));
+    ZG_CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_fb_accum, FB_ACC_THREADS, 0));
+    c->fb_ctas = (unsigned)std::max(1, sms * std::max(1, per_sm));
+    ZG_CK(cudaMalloc(&c->fb_gbuf, (size_t)c->fb_ctas * FB_BUCKETS * sizeof(XYZZ)));
+  }
   ZG_CK(cudaMalloc(&c->raw, c->max_blob + 16));
   ZG_CK(cudaMalloc(&c->enc, 3 * N * 32));
   ZG_CK(cudaMalloc(&c->T1, N * sizeof(Fr)));
   ZG_CK(cudaMalloc(&c->Bc, 2 * N * sizeof(Fr)));
-  ZG_CK(cudaMalloc(&c->win, 3 * (size_t)c->L * R * MSM_WINDOWS * sizeof(XYZZ)));
+  if (!c->fb) ZG_CK(cudaMalloc(&c->win, 3 * (size_t)c->L * R * MSM_WINDOWS * sizeof(XYZZ)));
   ZG_CK(cudaMalloc(&c->part, 3 * (size_t)c->L * R * sizeof(XYZZ)));
   ZG_CK(cudaMalloc(&c->nodes, 3 * (4 * R - 2) * sizeof(XYZZ)));
   ZG_CK(cudaMalloc(&c->amt, 3 * (4 * R - 2) * 64));
@@ -286,17 +321,16 @@ int build_seeded_params(zg_ctx* c, uint64_t seed) {
   for (int cs = 0; cs < 3; ++cs) {
     Fr tp = cs ? tau * coset_factor(ln, cs).inverse() : tau;
     k_powers<<<nblk(N, T), T, 0, s>>>(tp, pw, (uint32_t)N);
-    G1Aff* lines = c->bases + (size_t)cs * c->L * N;
     ntt4(c->tw, pw, tmp, sc, true, s);
     k_scale<<<nblk(N, T), T, 0, s>>>(sc, ninv, (uint32_t)N);
-    k_fixed_mul<<<nblk(N, T), T, 0, s>>>(tab, sc, lines + (size_t)c->lr * N, (uint32_t)N, ln);
+    k_fixed_mul<<<nblk(N, T), T, 0, s>>>(tab, sc, c->line_ptr(cs, c->lr), (uint32_t)N, ln);
     k_scale<<<nblk(N, T), T, 0, s>>>(sc, tau_hs, (uint32_t)N);
-    k_fixed_mul<<<nblk(N, T), T, 0, s>>>(tab, sc, lines + (size_t)(c->lr + 1) * N, (uint32_t)N, ln);
+    k_fixed_mul<<<nblk(N, T), T, 0, s>>>(tab, sc, c->line_ptr(cs, c->lr + 1), (uint32_t)N, ln);
     for (int d = 1; d <= c->lr; ++d) {
       k_quot_coeff<<<nblk(N, T), T, 0, s>>>(pw, coeff, (uint32_t)(N >> d), (uint32_t)N);
       ntt4(c->tw, coeff, tmp, sc, false, s);
       k_scale<<<nblk(N, T), T, 0, s>>>(sc, ninv, (uint32_t)N);
-      k_fixed_mul<<<nblk(N, T), T, 0, s>>>(tab, sc, lines + (size_t)(d - 1) * N, (uint32_t)N, ln);
+      k_fixed_mul<<<nblk(N, T), T, 0, s>>>(tab, sc, c->line_ptr(cs, d - 1), (uint32_t)N, ln);
     }
   }
   ZG_CK(cudaStreamSynchronize(s));
@@ -332,17 +366,16 @@ int load_mont_params(zg_ctx* c, const char* dir) {
     uint8_t hdr[6];
     bool ok = fread(hdr, 1, 6, f) == 6 && memcmp(hdr, "bamt", 4) == 0 && hdr[4] == ln && hdr[5] == c->lr;
     ok = ok && fseek(f, 256, SEEK_CUR) == 0;  // g2, high_g2 (uncompressed G2, 128 B each)
-    G1Aff* lines = c->bases + (size_t)cs * c->L * c->N;
     auto read_line = [&](G1Aff* dst) {
       if (fread(hostline.data(), 1, hostline.size(), f) != hostline.size()) return false;
       return cudaMemcpy(dst, hostline.data(), hostline.size(), cudaMemcpyHostToDevice) == cudaSuccess;
     };
-    ok = ok && read_line(lines + (size_t)c->lr * c->N);  // basis
-    for (int d = 0; ok && d < c->lr; ++d) ok = read_line(lines + (size_t)d * c->N);
+    ok = ok && read_line(c->line_ptr(cs, c->lr));  // basis
+    for (int d = 0; ok && d < c->lr; ++d) ok = read_line(c->line_ptr(cs, d));
     size_t van = 0;
     for (int d = 0; d < c->lr; ++d) van += (size_t)128 << (d + 1);
     ok = ok && fseek(f, (long)van, SEEK_CUR) == 0;
-    ok = ok && read_line(lines + (size_t)(c->lr + 1) * c->N);  // high_basis
+    ok = ok && read_line(c->line_ptr(cs, c->lr + 1));  // high_basis
     fclose(f);
     if (!ok) return fail(ZG_ERR_PARAMS, "malformed params file " + found);
   }
@@ -371,6 +404,11 @@ int merkle_levels(const uint8_t* items, size_t n_items, uint8_t* tree, const std
 int encode_device_locked(zg_ctx* c, const uint8_t* d_data, size_t len, cudaStream_t s) {
   const int lr = c->lr, lc = c->lc;
   const size_t R = c->R, C = c->C, N = c->N;
+  auto mark = [&](int k) {
+    if (c->profiling) cudaEventRecord(c->ev[k], s);
+  };
+  if (cudaStreamWaitEvent(s, c->done, 0) != cudaSuccess) return fail(ZG_ERR_CUDA, "stream wait failed");
+  mark(0);
   // RS extension: rows iNTT, column passes, rows NTT
   k_rows_from_raw<<<(unsigned)R, 256, C * sizeof(Fr) + 31 * C, s>>>(
       d_data, len, c->max_raw, lr, lc, c->enc, c->T1, c->tw.twi_c, c->tw.wni_lo, c->tw.wni_hi);
@@ -380,26 +418,49 @@ int encode_device_locked(zg_ctx* c, const uint8_t* d_data, size_t len, cudaStrea
   k_rows_ntt<<<dim3((unsigned)R, 2), 256, C * sizeof(Fr), s>>>(c->Bc, c->enc, lr, lc, c->tw.twf_c);
   int rc = check_launch();
   if (rc) return rc;
+  mark(1);
   // Merkle tree over the encoded data and the file root
   if ((rc = merkle_levels(c->enc, 3 * N, c->tree, c->tree_off, c->tree_depth, s))) return rc;
   k_file_root<<<1, 32, 0, s>>>(c->tree + c->tree_off[0], c->file_root);
-  // AMT: per-chunk MSMs, window combination, trees, serialisation
-  MsmChunkArgs a;
-  a.scalars = c->enc;
-  a.bases = c->bases;
-  a.win = c->win;
-  a.lr = lr;
-  a.lc = lc;
-  a.lines = c->L;
-  a.bitrev_rows = 1;
-  a.scalar_coset_stride = N;
-  a.base_coset_stride = (uint64_t)c->L * N;
-  k_msm_chunks<<<dim3((unsigned)R, 3), MSM_THREADS, msm_smem_bytes(lc), s>>>(a);
-  const uint32_t nmsm = (uint32_t)(3 * c->L * R);
-  k_msm_combine<<<nblk(nmsm, 64), 64, 0, s>>>(c->win, c->part, nmsm);
-  k_amt_tree<<<dim3((unsigned)c->L, 3), 512, 0, s>>>(c->part, c->nodes, lr, c->L);
+  mark(2);
+  // AMT: per-chunk MSMs, trees, serialisation
+  if (c->fb) {
+    k_fb_sort<<<dim3((unsigned)R, 3), 256, fb_sort_smem_bytes(lc), s>>>(c->enc, c->fb_offs, c->fb_ents, lr, lc, 1,
+                                                                         N);
+    FbAccArgs fa;
+    fa.tab = c->tab;
+    fa.offs = c->fb_offs;
+    fa.ents = c->fb_ents;
+    fa.outT = c->fb_T;
+    fa.outS = c->fb_S;
+    fa.lr = lr;
+    fa.lc = lc;
+    fa.lines = c->L;
+    const uint32_t units = (uint32_t)(3 * R * c->L);
+    k_fb_accum<<<std::min<unsigned>(c->fb_ctas, units), FB_ACC_THREADS, 0, s>>>(fa, c->fb_gbuf, units);
+    mark(3);
+    k_fb_combine<<<nblk(units, 64), 64, 0, s>>>(c->fb_T, c->fb_S, c->part, lr, c->L, units);
+  } else {
+    MsmChunkArgs a;
+    a.scalars = c->enc;
+    a.bases = c->tab;
+    a.win = c->win;
+    a.lr = lr;
+    a.lc = lc;
+    a.lines = c->L;
+    a.bitrev_rows = 1;
+    a.scalar_coset_stride = N;
+    a.base_coset_stride = (uint64_t)c->L * c->W * N;
+    a.base_line_stride = (uint64_t)c->W * N;
+    k_msm_chunks<<<dim3((unsigned)R, 3), MSM_THREADS, msm_smem_bytes(lc), s>>>(a);
+    mark(3);
+    const uint32_t nmsm = (uint32_t)(3 * c->L * R);
+    k_msm_combine<<<nblk(nmsm, 64), 64, 0, s>>>(c->win, c->part, nmsm);
+  }
+  k_amt_tree<<<dim3((unsigned)c->L, 3), 256, 0, s>>>(c->part, c->nodes, lr, c->L);
   const uint32_t nn = (uint32_t)(3 * (4 * R - 2));
   k_serialize_nodes<<<nblk(nn, 128), 128, 0, s>>>(c->nodes, c->amt, nn);
+  mark(4);
   SliceArgs sa;
   sa.enc = c->enc;
   sa.amt = c->amt;
@@ -410,6 +471,11 @@ int encode_device_locked(zg_ctx* c, const uint8_t* d_data, size_t len, cudaStrea
   sa.lc = lc;
   sa.slice_size = c->slice_size;
   k_slices<<<(unsigned)(3 * R), 256, 0, s>>>(sa);
+  mark(5);
+  // 3 RS passes, leaves + tree_depth parent levels, file root, MSM (sort,
+  // accumulate, combine or chunks, combine), trees, serialisation, slices
+  c->launches += 3 + (uint64_t)c->tree_depth + 1 + 1 + (c->fb ? 3 : 2) + 1 + 1 + 1;
+  if (cudaEventRecord(c->done, s) != cudaSuccess) return fail(ZG_ERR_CUDA, "event record failed");
   return check_launch();
 }
 
@@ -441,7 +507,7 @@ __global__ void k_mont_to_canon(Fr* v, uint64_t n, Fr scale, int do_scale) {
   v[i] = x.to_canonical();
 }
 // single-CTA transform of each contiguous vector (n <= 2048)
-__global__ void k_ntt_small(Fr* v, int logn, const Fr* tw) {
+__global__ void __launch_bounds__(256) k_ntt_small(Fr* v, int logn, const Fr* tw) {
   extern __shared__ __align__(16) uint8_t smem[];
   Fr* s = reinterpret_cast<Fr*>(smem);
   const int n = 1 << logn;
@@ -479,18 +545,29 @@ __global__ void k_selftest(const Fq* a, const Fq* b, Fq* res, uint32_t n) {
 }
 
 
-__global__ void k_echo(Fr a, uint64_t pad, Fr b, int flag, Fr* out, const Fr* pa) {
-  if (threadIdx.x != 0 || blockIdx.x != 0) return;
-  out[0] = a;
-  out[1] = b;
-  out[2] = a * b;
-  out[3] = pa[0] * pa[1];
-  out[4] = pa[0];
-  Fr c = pa[1];
-  out[5] = a * c;
-  out[6] = c * a;
-  out[7] = Fr::mul(pa[1], a);
-  (void)pad; (void)flag;
+
+
+// independent 32-bit multiply-add chains: the integer multiply throughput the
+// Montgomery products are built from
+__global__ void k_imad_probe(uint32_t* sink, uint32_t iters, uint32_t seed) {
+  uint32_t a0 = seed + threadIdx.x, a1 = a0 ^ 0x9e3779b9u, a2 = a0 + 0x7f4a7c15u, a3 = a0 * 3u,
+           a4 = a0 ^ 0x85ebca6bu, a5 = a0 + 0xc2b2ae35u, a6 = a0 * 5u, a7 = a0 ^ 0x27d4eb2fu;
+  const uint32_t m = seed | 1u, k = seed ^ 0x5bd1e995u;
+  for (uint32_t i = 0; i < iters; ++i) {
+#pragma unroll
+    for (int u = 0; u < 16; ++u) {
+      asm volatile("mad.lo.u32 %0, %0, %1, %2;" : "+r"(a0) : "r"(m), "r"(k));
+      asm volatile("mad.lo.u32 %0, %0, %1, %2;" : "+r"(a1) : "r"(m), "r"(k));
+      asm volatile("mad.lo.u32 %0, %0, %1, %2;" : "+r"(a2) : "r"(m), "r"(k));
+      asm volatile("mad.lo.u32 %0, %0, %1, %2;" : "+r"(a3) : "r"(m), "r"(k));
+      asm volatile("mad.lo.u32 %0, %0, %1, %2;" : "+r"(a4) : "r"(m), "r"(k));
+      asm volatile("mad.lo.u32 %0, %0, %1, %2;" : "+r"(a5) : "r"(m), "r"(k));
+      asm volatile("mad.lo.u32 %0, %0, %1, %2;" : "+r"(a6) : "r"(m), "r"(k));
+      asm volatile("mad.lo.u32 %0, %0, %1, %2;" : "+r"(a7) : "r"(m), "r"(k));
+    }
+  }
+  uint32_t x = a0 ^ a1 ^ a2 ^ a3 ^ a4 ^ a5 ^ a6 ^ a7;
+  if (x == 0x12345678u) sink[0] = x;
 }
 
 }  // namespace
@@ -523,13 +600,36 @@ int zg_ctx_create(const zg_config* cfg, zg_ctx** out) {
   if ((rc = set_smem_limits())) return bail(rc);
   if (cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking) != cudaSuccess)
     return bail(fail(ZG_ERR_CUDA, "stream create failed"));
+  if (cudaEventCreateWithFlags(&c->done, cudaEventDisableTiming) != cudaSuccess ||
+      cudaEventRecord(c->done, c->stream) != cudaSuccess)
+    return bail(fail(ZG_ERR_CUDA, "event create failed"));
   if ((rc = make_twiddles(c->lr, c->lc, &c->tw))) return bail(rc);
-  if (cudaMalloc(&c->bases, (size_t)3 * c->L * c->N * sizeof(G1Aff)) != cudaSuccess)
+  // MSM variant: fixed-base windows (tables of 24 multiples per param point)
+  // unless 8-bit windows are requested or the tables do not fit
+  const uint32_t wb = cfg->msm_window_bits;
+  if (wb != 0 && wb != 8 && wb != (uint32_t)FB_BITS)
+    return bail(fail(ZG_ERR_INVALID_ARG, "msm_window_bits must be 0, 8 or 11"));
+  c->fb = (wb == 0 || wb == (uint32_t)FB_BITS) && c->lc <= 10;
+  c->W = c->fb ? FB_WINDOWS : 1;
+  if (c->fb && cudaMalloc(&c->tab, (size_t)3 * c->L * c->W * c->N * sizeof(G1Aff)) != cudaSuccess) {
+    cudaGetLastError();
+    if (wb == (uint32_t)FB_BITS) return bail(fail(ZG_ERR_CUDA, "cannot allocate fixed-base tables"));
+    c->fb = false;
+    c->W = 1;
+    c->tab = nullptr;
+  }
+  if (!c->tab && cudaMalloc(&c->tab, (size_t)3 * c->L * c->N * sizeof(G1Aff)) != cudaSuccess)
     return bail(fail(ZG_ERR_CUDA, "cannot allocate params"));
   if ((rc = alloc_blob_buffers(c))) return bail(rc);
   if (cfg->params_dir && cfg->params_dir[0]) rc = load_mont_params(c, cfg->params_dir);
   else rc = build_seeded_params(c, cfg->tau_seed);
   if (rc) return bail(rc);
+  if (c->fb) {
+    const uint64_t nl = (uint64_t)3 * c->L;
+    k_fb_tables<<<nblk(nl * c->N, 128), 128, 0, c->stream>>>(c->tab, c->N, nl);
+    if (cudaStreamSynchronize(c->stream) != cudaSuccess || cudaGetLastError() != cudaSuccess)
+      return bail(fail(ZG_ERR_CUDA, "fixed-base table build failed"));
+  }
   *out = c;
   return ZG_OK;
 }
@@ -537,12 +637,15 @@ int zg_ctx_create(const zg_config* cfg, zg_ctx** out) {
 void zg_ctx_destroy(zg_ctx* c) {
   if (!c) return;
   cudaSetDevice(c->device);
+  if (c->done) cudaEventSynchronize(c->done);  // work queued on caller streams
   if (c->stream) cudaStreamSynchronize(c->stream);
   free_twiddles(&c->tw);
-  void* ps[] = {c->bases, c->raw, c->enc, c->T1, c->Bc, c->win, c->part, c->nodes, c->amt,
-                c->tree, c->tree_off_d, c->slices, c->file_root};
+  void* ps[] = {c->tab, c->raw, c->enc, c->T1, c->Bc, c->win, c->part, c->nodes, c->amt,
+                c->tree, c->tree_off_d, c->slices, c->file_root, c->fb_offs, c->fb_ents, c->fb_T, c->fb_S, c->fb_gbuf};
   for (void* p : ps) if (p) cudaFree(p);
   if (c->h_in) cudaFreeHost(c->h_in);
+  for (cudaEvent_t e : c->ev) if (e) cudaEventDestroy(e);
+  if (c->done) cudaEventDestroy(c->done);
   if (c->stream) cudaStreamDestroy(c->stream);
   delete c;
 }
@@ -593,8 +696,16 @@ int zg_encode(zg_ctx* c, const uint8_t* data, size_t len, int require_data, zg_r
     if (cudaMallocHost(&r->data, r->data_len) != cudaSuccess)
       return bail(fail(ZG_ERR_CUDA, "cannot allocate pinned reply"));
   }
-  if (len) memcpy(c->h_in, data, len);
-  if (len && cudaMemcpyAsync(c->raw, c->h_in, len, cudaMemcpyHostToDevice, s) != cudaSuccess)
+  // page-locked caller buffers are copied by DMA directly; pageable ones go
+  // through the context's pinned staging buffer
+  const uint8_t* src = data;
+  cudaPointerAttributes pa;
+  if (len && (cudaPointerGetAttributes(&pa, data) != cudaSuccess || pa.type != cudaMemoryTypeHost)) {
+    cudaGetLastError();
+    memcpy(c->h_in, data, len);
+    src = c->h_in;
+  }
+  if (len && cudaMemcpyAsync(c->raw, src, len, cudaMemcpyHostToDevice, s) != cudaSuccess)
     return bail(fail(ZG_ERR_CUDA, "H2D copy failed"));
   int rc = encode_device_locked(c, c->raw, len, s);
   if (rc) return bail(rc);
@@ -666,15 +777,38 @@ const uint8_t* zg_reply_roots(const zg_reply* r, size_t* len) {
   return r->roots;
 }
 
-int zg_ctx_param_line(zg_ctx* c, int coset, int line, uint8_t* host_out, size_t cap) {
-  if (!c || coset < 0 || coset > 2 || line < 0 || line >= c->L) return fail(ZG_ERR_INVALID_ARG, "bad line");
-  size_t bytes = c->N * sizeof(G1Aff);
+int zg_ctx_param_points(zg_ctx* c, int coset, int line, size_t first, size_t count, uint8_t* host_out,
+                        size_t cap) {
+  if (!c || coset < 0 || coset > 2 || line < 0 || line >= c->L || first > c->N || count > c->N - first)
+    return fail(ZG_ERR_INVALID_ARG, "bad param range");
+  size_t bytes = count * sizeof(G1Aff);
   if (cap < bytes) return fail(ZG_ERR_INVALID_ARG, "buffer too small");
   std::lock_guard<std::mutex> g(c->mu);
   ZG_CK(cudaSetDevice(c->device));
-  ZG_CK(cudaMemcpy(host_out, c->bases + ((size_t)coset * c->L + line) * c->N, bytes, cudaMemcpyDeviceToHost));
+  ZG_CK(cudaMemcpy(host_out, c->line_ptr(coset, line) + first, bytes, cudaMemcpyDeviceToHost));
   return ZG_OK;
 }
+
+int zg_ctx_set_profiling(zg_ctx* c, int enable) {
+  if (!c) return fail(ZG_ERR_INVALID_ARG, "null context");
+  std::lock_guard<std::mutex> g(c->mu);
+  ZG_CK(cudaSetDevice(c->device));
+  if (enable && !c->ev[0])
+    for (cudaEvent_t& e : c->ev) ZG_CK(cudaEventCreate(&e));
+  c->profiling = enable != 0;
+  return ZG_OK;
+}
+
+int zg_ctx_phase_times(zg_ctx* c, float* ms, int n) {
+  if (!c || !ms || !c->ev[0]) return fail(ZG_ERR_INVALID_ARG, "profiling not enabled");
+  std::lock_guard<std::mutex> g(c->mu);
+  ZG_CK(cudaSetDevice(c->device));
+  ZG_CK(cudaEventSynchronize(c->ev[5]));
+  for (int k = 0; k < 5 && k < n; ++k) ZG_CK(cudaEventElapsedTime(&ms[k], c->ev[k], c->ev[k + 1]));
+  return ZG_OK;
+}
+
+uint64_t zg_ctx_launches(const zg_ctx* c) { return c ? c->launches : 0; }
 
 int zg_msm_chunks(const void* d_bases, const void* d_scalars, uint32_t lines, uint32_t log_nchunks,
                   uint32_t log_chunk, void* d_out, void* stream) {
@@ -698,6 +832,7 @@ int zg_msm_chunks(const void* d_bases, const void* d_scalars, uint32_t lines, ui
   a.bitrev_rows = 0;
   a.scalar_coset_stride = 0;
   a.base_coset_stride = 0;
+  a.base_line_stride = (uint64_t)nch << log_chunk;
   k_msm_chunks<<<dim3((unsigned)nch, 1), MSM_THREADS, msm_smem_bytes((int)log_chunk), s>>>(a);
   k_msm_combine<<<nblk(count, 64), 64, 0, s>>>(win, part, (uint32_t)count);
   k_serialize_nodes<<<nblk(count, 128), 128, 0, s>>>(part, (uint8_t*)d_out, (uint32_t)count);
@@ -797,23 +932,33 @@ int zg_selftest(int* fails, int nops) {
 }
 
 
-int zg_debug_echo(uint8_t* host_out) {  // host_out: 11 x 32 B
-  Fr a = host_fr_from_u32(32).inverse(), b = coset_factor(5, 1);
-  Fr* d = nullptr;
-  ZG_CK(cudaMalloc(&d, 16 * sizeof(Fr)));
-  Fr ab[2] = {a, b};
-  ZG_CK(cudaMemcpy(d + 12, ab, 2 * sizeof(Fr), cudaMemcpyHostToDevice));
-  k_echo<<<1, 32>>>(a, 77, b, 1, d, d + 12);
-  // k_mont_to_canon on [b, b] with scale a
-  ZG_CK(cudaMemcpy(d + 8, ab + 1, sizeof(Fr), cudaMemcpyHostToDevice));
-  ZG_CK(cudaMemcpy(d + 9, ab + 1, sizeof(Fr), cudaMemcpyHostToDevice));
-  k_mont_to_canon<<<1, 32>>>(d + 8, 2, a, 1);
-  ZG_CK(cudaDeviceSynchronize());
-  ZG_CK(cudaMemcpy(host_out, d, 10 * sizeof(Fr), cudaMemcpyDeviceToHost));
-  Fr ref = (b * a).to_canonical();
-  memcpy(host_out + 10 * 32, &ref, 32);
-  cudaFree(d);
-  return 0;
+
+
+int zg_probe_imad(int device, double* gimad_per_s) {
+  if (!gimad_per_s) return fail(ZG_ERR_INVALID_ARG, "null output");
+  ZG_CK(cudaSetDevice(device));
+  int sms = 0;
+  ZG_CK(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device));
+  uint32_t* sink = nullptr;
+  ZG_CK(cudaMalloc(&sink, 4));
+  cudaEvent_t e0, e1;
+  ZG_CK(cudaEventCreate(&e0));
+  ZG_CK(cudaEventCreate(&e1));
+  const unsigned blocks = (unsigned)sms * 8, threads = 256;
+  const uint32_t iters = 4096;
+  k_imad_probe<<<blocks, threads>>>(sink, 64, 7);  // warm-up
+  ZG_CK(cudaEventRecord(e0));
+  k_imad_probe<<<blocks, threads>>>(sink, iters, 7);
+  ZG_CK(cudaEventRecord(e1));
+  ZG_CK(cudaEventSynchronize(e1));
+  float ms = 0;
+  ZG_CK(cudaEventElapsedTime(&ms, e0, e1));
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  cudaFree(sink);
+  double ops = (double)blocks * threads * iters * 16 * 8;
+  *gimad_per_s = ops / (ms * 1e-3) / 1e9;
+  return ZG_OK;
 }
 
 int zg_merkle_roots(const void* d_items, size_t n_items, void* d_roots, void* stream) {

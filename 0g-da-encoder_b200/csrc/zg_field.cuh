@@ -261,6 +261,92 @@ struct Fp {
 #endif
   }
 
+  // two independent products r1 = a*b, r2 = c*d with their CIOS rows
+  // interleaved: the two carry chains have no data dependence, so either
+  // fills the other's multiply latency.
+  ZG_HD static void mul2(const Fp& a, const Fp& b, const Fp& c, const Fp& d, Fp& r1, Fp& r2) {
+#ifdef __CUDA_ARCH__
+    uint32_t t0 = 0, t1 = 0, t2 = 0, t3 = 0, t4 = 0, t5 = 0, t6 = 0, t7 = 0, t8 = 0;
+    uint32_t u0 = 0, u1 = 0, u2 = 0, u3 = 0, u4 = 0, u5 = 0, u6 = 0, u7 = 0, u8 = 0;
+#pragma unroll
+    for (int i = 0; i < 8; ++i) {
+      row_mac(t0, t1, t2, t3, t4, t5, t6, t7, t8, a, b.v[i]);
+      row_mac(u0, u1, u2, u3, u4, u5, u6, u7, u8, c, d.v[i]);
+      const uint32_t m = t0 * C::inv;
+      const uint32_t n = u0 * C::inv;
+      row_red(t0, t1, t2, t3, t4, t5, t6, t7, t8, m);
+      row_red(u0, u1, u2, u3, u4, u5, u6, u7, u8, n);
+      t0 = t1; t1 = t2; t2 = t3; t3 = t4; t4 = t5; t5 = t6; t6 = t7; t7 = t8;
+      u0 = u1; u1 = u2; u2 = u3; u3 = u4; u4 = u5; u5 = u6; u6 = u7; u7 = u8;
+    }
+    Fp x, y;
+    x.v[0] = t0; x.v[1] = t1; x.v[2] = t2; x.v[3] = t3; x.v[4] = t4; x.v[5] = t5; x.v[6] = t6; x.v[7] = t7;
+    y.v[0] = u0; y.v[1] = u1; y.v[2] = u2; y.v[3] = u3; y.v[4] = u4; y.v[5] = u5; y.v[6] = u6; y.v[7] = u7;
+    Fp xs, ys;
+    uint32_t bx = sub_raw(xs, x, modulus());
+    uint32_t by = sub_raw(ys, y, modulus());
+    r1 = bx ? x : xs;
+    r2 = by ? y : ys;
+#else
+    Fp x = mul(a, b), y = mul(c, d);
+    r1 = x;
+    r2 = y;
+#endif
+  }
+
+#ifdef __CUDA_ARCH__
+  // t[0..8] = t[0..7] + a * bi (even limbs chain, then odd limbs chain)
+  __device__ __forceinline__ static void row_mac(uint32_t& t0, uint32_t& t1, uint32_t& t2, uint32_t& t3,
+                                                 uint32_t& t4, uint32_t& t5, uint32_t& t6, uint32_t& t7,
+                                                 uint32_t& t8, const Fp& a, uint32_t bi) {
+    asm("mad.lo.cc.u32 %0, %9, %17, %0;\n\t"
+        "madc.hi.cc.u32 %1, %9, %17, %1;\n\t"
+        "madc.lo.cc.u32 %2, %11, %17, %2;\n\t"
+        "madc.hi.cc.u32 %3, %11, %17, %3;\n\t"
+        "madc.lo.cc.u32 %4, %13, %17, %4;\n\t"
+        "madc.hi.cc.u32 %5, %13, %17, %5;\n\t"
+        "madc.lo.cc.u32 %6, %15, %17, %6;\n\t"
+        "madc.hi.cc.u32 %7, %15, %17, %7;\n\t"
+        "addc.u32 %8, 0, 0;\n\t"
+        "mad.lo.cc.u32 %1, %10, %17, %1;\n\t"
+        "madc.hi.cc.u32 %2, %10, %17, %2;\n\t"
+        "madc.lo.cc.u32 %3, %12, %17, %3;\n\t"
+        "madc.hi.cc.u32 %4, %12, %17, %4;\n\t"
+        "madc.lo.cc.u32 %5, %14, %17, %5;\n\t"
+        "madc.hi.cc.u32 %6, %14, %17, %6;\n\t"
+        "madc.lo.cc.u32 %7, %16, %17, %7;\n\t"
+        "madc.hi.u32 %8, %16, %17, %8;"
+        : "+r"(t0), "+r"(t1), "+r"(t2), "+r"(t3), "+r"(t4), "+r"(t5), "+r"(t6), "+r"(t7), "+r"(t8)
+        : "r"(a.v[0]), "r"(a.v[1]), "r"(a.v[2]), "r"(a.v[3]), "r"(a.v[4]), "r"(a.v[5]), "r"(a.v[6]),
+          "r"(a.v[7]), "r"(bi));
+  }
+  // t[0..8] += m * p
+  __device__ __forceinline__ static void row_red(uint32_t& t0, uint32_t& t1, uint32_t& t2, uint32_t& t3,
+                                                 uint32_t& t4, uint32_t& t5, uint32_t& t6, uint32_t& t7,
+                                                 uint32_t& t8, uint32_t m) {
+    asm("mad.lo.cc.u32 %0, %9, %10, %0;\n\t"
+        "madc.hi.cc.u32 %1, %9, %10, %1;\n\t"
+        "madc.lo.cc.u32 %2, %9, %12, %2;\n\t"
+        "madc.hi.cc.u32 %3, %9, %12, %3;\n\t"
+        "madc.lo.cc.u32 %4, %9, %14, %4;\n\t"
+        "madc.hi.cc.u32 %5, %9, %14, %5;\n\t"
+        "madc.lo.cc.u32 %6, %9, %16, %6;\n\t"
+        "madc.hi.cc.u32 %7, %9, %16, %7;\n\t"
+        "addc.u32 %8, %8, 0;\n\t"
+        "mad.lo.cc.u32 %1, %9, %11, %1;\n\t"
+        "madc.hi.cc.u32 %2, %9, %11, %2;\n\t"
+        "madc.lo.cc.u32 %3, %9, %13, %3;\n\t"
+        "madc.hi.cc.u32 %4, %9, %13, %4;\n\t"
+        "madc.lo.cc.u32 %5, %9, %15, %5;\n\t"
+        "madc.hi.cc.u32 %6, %9, %15, %6;\n\t"
+        "madc.lo.cc.u32 %7, %9, %17, %7;\n\t"
+        "madc.hi.u32 %8, %9, %17, %8;"
+        : "+r"(t0), "+r"(t1), "+r"(t2), "+r"(t3), "+r"(t4), "+r"(t5), "+r"(t6), "+r"(t7), "+r"(t8)
+        : "r"(m), "r"(C::p0), "r"(C::p1), "r"(C::p2), "r"(C::p3), "r"(C::p4), "r"(C::p5), "r"(C::p6),
+          "r"(C::p7));
+  }
+#endif
+
   // same as mul with the modulus limbs as instruction immediates (diagnostic)
   ZG_HD static Fp mul_imm(const Fp& a, const Fp& b) {
 #ifdef __CUDA_ARCH__

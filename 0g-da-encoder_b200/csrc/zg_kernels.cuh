@@ -71,7 +71,7 @@ __device__ __forceinline__ Fr pow_split(const Fr* lo, const Fr* hi, uint32_t e, 
 // D[r][j] is the Fr of the 31-byte chunk r*C + j of the zero-padded RawData
 // whose last four bytes hold the payload length (raw_data.rs:55-73,
 // raw_blob.rs:33-40).
-__global__ void k_rows_from_raw(const uint8_t* __restrict__ raw, uint64_t len, uint64_t max_raw, int lr, int lc,
+__global__ void __launch_bounds__(256) k_rows_from_raw(const uint8_t* __restrict__ raw, uint64_t len, uint64_t max_raw, int lr, int lc,
                                 uint8_t* __restrict__ enc0, Fr* __restrict__ T1, const Fr* __restrict__ twi_c,
                                 const Fr* __restrict__ wni_lo, const Fr* __restrict__ wni_hi) {
   extern __shared__ __align__(16) uint8_t smem[];
@@ -118,7 +118,7 @@ __global__ void k_rows_from_raw(const uint8_t* __restrict__ raw, uint64_t len, u
 // c in {1, 2}: scale coefficient m = s + C q by g_c^m / N, forward NTT over q,
 // multiply by w_N^{s r}; store Bc[c-1][r][s].
 constexpr int COLS_PER_BLOCK = 2;
-__global__ void k_cols(const Fr* __restrict__ T1, Fr* __restrict__ Bc, int lr, int lc,
+__global__ void __launch_bounds__(256) k_cols(const Fr* __restrict__ T1, Fr* __restrict__ Bc, int lr, int lc,
                        const Fr* __restrict__ twi_r, const Fr* __restrict__ twf_r,
                        const Fr* __restrict__ gs_lo, const Fr* __restrict__ gs_hi,
                        const Fr* __restrict__ wn_lo, const Fr* __restrict__ wn_hi) {
@@ -151,7 +151,7 @@ __global__ void k_cols(const Fr* __restrict__ T1, Fr* __restrict__ Bc, int lr, i
 
 // Pass 3: per coset c in {1,2} and row r, forward NTT over s (size C):
 // enc[c][r][j] = canonical( sum_s v_C^{s j} Bc[c-1][r][s] ).
-__global__ void k_rows_ntt(const Fr* __restrict__ Bc, uint8_t* __restrict__ enc, int lr, int lc,
+__global__ void __launch_bounds__(256) k_rows_ntt(const Fr* __restrict__ Bc, uint8_t* __restrict__ enc, int lr, int lc,
                            const Fr* __restrict__ twf_c) {
   extern __shared__ __align__(16) uint8_t smem[];
   const int R = 1 << lr, C = 1 << lc;
@@ -234,12 +234,12 @@ struct MsmChunkArgs {
   int bitrev_rows;         // 1: chunk b reads encoded row bitrev(b), column bitrev(t)
   uint64_t scalar_coset_stride;  // scalars between cosets (elements)
   uint64_t base_coset_stride;    // bases between cosets (points)
+  uint64_t base_line_stride;     // bases between lines (points)
 };
 
 __global__ void __launch_bounds__(MSM_THREADS, 1) k_msm_chunks(MsmChunkArgs a) {
   extern __shared__ __align__(16) uint8_t smem[];
   const int C = 1 << a.lc;
-  const int N = 1 << (a.lr + a.lc);
   const uint32_t b = blockIdx.x, coset = blockIdx.y;
   // smem: scalars [C][8] u32 | lists [32][C] u16 | offs [32][129] u16 | cnt [129] u32
   uint32_t* scal = reinterpret_cast<uint32_t*>(smem);
@@ -312,7 +312,8 @@ __global__ void __launch_bounds__(MSM_THREADS, 1) k_msm_chunks(MsmChunkArgs a) {
   for (int l0 = 0; l0 < a.lines; l0 += MSM_LINES_PER_PASS) {
     const int l = l0 + li;
     const bool active = l < a.lines;
-    const G1Aff* bl = a.bases + a.base_coset_stride * coset + (size_t)(active ? l : 0) * N + (size_t)b * C;
+    const G1Aff* bl = a.bases + a.base_coset_stride * coset + (size_t)(active ? l : 0) * a.base_line_stride +
+                      (size_t)b * C;
     XYZZ run = XYZZ::inf(), acc = XYZZ::inf();
     if (active) {
       for (int k = 64 * g + 64; k > 64 * g; --k) {
@@ -341,8 +342,248 @@ __global__ void __launch_bounds__(MSM_THREADS, 1) k_msm_chunks(MsmChunkArgs a) {
   }
 }
 
+
+// ---------------------------------------------------------------------------
+// MSM with fixed-base windows. The params never change, so every base P is
+// stored with its window multiples T_w = 2^{11 w} P (w < 24): a chunk MSM
+//   sum_t s_t P_t = sum_t sum_w d_{t,w} T_w[t]
+// over the signed 11-bit digits d of the scalars is one bucket accumulation
+// (buckets |d| = 1..1024) with no doublings. Per chunk: ~24 x 1024 mixed adds
+// plus 2 x 1024 bucket-reduction adds, against 32 x (1024 + 256) for 8-bit
+// windows with doublings.
+constexpr int FB_BITS = 11;
+constexpr int FB_WINDOWS = 24;                    // ceil((254 + 1) / 11)
+constexpr int FB_BUCKETS = 1 << (FB_BITS - 1);    // 1024
+constexpr int FB_ACC_THREADS = 128;
+constexpr int FB_PER_THREAD = FB_BUCKETS / FB_ACC_THREADS;  // 8 buckets per thread
+
+// window w's multiples: tab[(line * W + w) * N + p]; window 0 already holds the
+// bases. One thread per (line, point): 11 doublings per window, then one
+// batch inversion for the 23 affine conversions.
+__global__ void __launch_bounds__(128) k_fb_tables(G1Aff* tab, uint64_t N, uint64_t nlines) {
+  uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= nlines * N) return;
+  const uint64_t line = i / N, p = i % N;
+  G1Aff* col = tab + line * FB_WINDOWS * N + p;
+  XYZZ pts[FB_WINDOWS - 1];
+  XYZZ acc = XYZZ::from_affine(col[0]);
+  for (int w = 1; w < FB_WINDOWS; ++w) {
+#pragma unroll 1
+    for (int k = 0; k < FB_BITS; ++k) acc = acc.dbl();
+    pts[w - 1] = acc;
+  }
+  // batch inversion of the ZZZ coordinates (bases are never infinity)
+  Fq pre[FB_WINDOWS - 1];
+  Fq run = Fq::one();
+  for (int w = 0; w < FB_WINDOWS - 1; ++w) {
+    pre[w] = run;
+    run = ZG_FMUL(run, pts[w].ZZZ);
+  }
+  Fq inv = run.inverse();
+  for (int w = FB_WINDOWS - 2; w >= 0; --w) {
+    Fq izzz = ZG_FMUL(inv, pre[w]);
+    inv = ZG_FMUL(inv, pts[w].ZZZ);
+    Fq izz = ZG_FMUL(ZG_FMUL(pts[w].ZZ, pts[w].ZZ), ZG_FMUL(izzz, izzz));
+    G1Aff a;
+    a.x = ZG_FMUL(pts[w].X, izz);
+    a.y = ZG_FMUL(pts[w].Y, izzz);
+    col[(uint64_t)(w + 1) * N] = a;
+  }
+}
+
+// signed 11-bit digit w of a scalar given as 8 little-endian u32 limbs
+__device__ __forceinline__ uint32_t fb_window_bits(const uint32_t* s, int w) {
+  const int o = FB_BITS * w;
+  const int li = o >> 5, sh = o & 31;
+  uint32_t v = s[li] >> sh;
+  if (sh > 32 - FB_BITS && li + 1 < 8) v |= s[li + 1] << (32 - sh);
+  return v & ((1u << FB_BITS) - 1);
+}
+
+// Per chunk: counting sort of the (point, window) pairs by |digit|.
+//   offs[g][k-1] .. offs[g][k]  = entries of bucket k (k = 1..1024)
+//   ents[g][e] = t | w << 10 | sign << 15
+// g = coset * nchunks + chunk. Chunk b reads encoded row bitrev(b), element t
+// = column bitrev(t) when bitrev_rows is set (HalfBlob::generate's index_reverse).
+__global__ void __launch_bounds__(256) k_fb_sort(const uint8_t* __restrict__ scalars, uint32_t* __restrict__ offs,
+                                                 uint16_t* __restrict__ ents, int lr, int lc, int bitrev_rows,
+                                                 uint64_t scalar_coset_stride) {
+  extern __shared__ __align__(16) uint8_t smem[];
+  const int C = 1 << lc;
+  const uint32_t b = blockIdx.x, coset = blockIdx.y;
+  const uint32_t g = coset * (1u << lr) + b;
+  uint32_t* scal = reinterpret_cast<uint32_t*>(smem);            // [C][8]
+  uint32_t* cnt = scal + (size_t)C * 8;                           // [FB_BUCKETS + 1]
+  uint32_t* part = cnt + FB_BUCKETS + 1;                          // [256]
+  uint16_t* lst = reinterpret_cast<uint16_t*>(part + 256);        // [W * C]
+  const uint32_t row = bitrev_rows ? brev_bits(b, lr) : b;
+  const uint8_t* src = scalars + (scalar_coset_stride * coset + (uint64_t)row * C) * 32;
+  for (int t = threadIdx.x; t < C; t += blockDim.x) {
+    uint32_t col = bitrev_rows ? brev_bits(t, lc) : t;
+    const uint4* q = reinterpret_cast<const uint4*>(src + (size_t)col * 32);
+    uint4 x = q[0], y = q[1];
+    uint32_t* d = scal + (size_t)t * 8;
+    d[0] = x.x; d[1] = x.y; d[2] = x.z; d[3] = x.w; d[4] = y.x; d[5] = y.y; d[6] = y.z; d[7] = y.w;
+  }
+  for (int k = threadIdx.x; k <= FB_BUCKETS; k += blockDim.x) cnt[k] = 0;
+  __syncthreads();
+  // pass 1: counts
+  for (int t = threadIdx.x; t < C; t += blockDim.x) {
+    const uint32_t* s = scal + (size_t)t * 8;
+    uint32_t carry = 0;
+    for (int w = 0; w < FB_WINDOWS; ++w) {
+      uint32_t v = fb_window_bits(s, w) + carry;
+      int d;
+      if (v >= (uint32_t)FB_BUCKETS) { d = (int)v - (1 << FB_BITS); carry = 1; }
+      else { d = (int)v; carry = 0; }
+      if (d) atomicAdd(&cnt[d < 0 ? -d : d], 1u);
+    }
+  }
+  __syncthreads();
+  // exclusive scan of cnt[1..1024] in 256 blocks of 4
+  {
+    const int k0 = 1 + 4 * threadIdx.x;
+    uint32_t s4 = 0;
+    for (int k = k0; k < k0 + 4; ++k) s4 += cnt[k];
+    part[threadIdx.x] = s4;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      uint32_t acc = 0;
+      for (int i = 0; i < 256; ++i) { uint32_t v = part[i]; part[i] = acc; acc += v; }
+    }
+    __syncthreads();
+    uint32_t acc = part[threadIdx.x];
+    for (int k = k0; k < k0 + 4; ++k) {
+      uint32_t v = cnt[k];
+      cnt[k] = acc;            // becomes the fill pointer of bucket k
+      offs[(size_t)g * (FB_BUCKETS + 1) + k - 1] = acc;
+      acc += v;
+    }
+    if (threadIdx.x == blockDim.x - 1) offs[(size_t)g * (FB_BUCKETS + 1) + FB_BUCKETS] = acc;
+  }
+  __syncthreads();
+  // pass 2: scatter
+  for (int t = threadIdx.x; t < C; t += blockDim.x) {
+    const uint32_t* s = scal + (size_t)t * 8;
+    uint32_t carry = 0;
+    for (int w = 0; w < FB_WINDOWS; ++w) {
+      uint32_t v = fb_window_bits(s, w) + carry;
+      int d;
+      if (v >= (uint32_t)FB_BUCKETS) { d = (int)v - (1 << FB_BITS); carry = 1; }
+      else { d = (int)v; carry = 0; }
+      if (d) {
+        uint32_t pos = atomicAdd(&cnt[d < 0 ? -d : d], 1u);
+        lst[pos] = (uint16_t)(t | (w << 10) | (d < 0 ? 0x8000 : 0));
+      }
+    }
+  }
+  __syncthreads();
+  const uint32_t total = offs[(size_t)g * (FB_BUCKETS + 1) + FB_BUCKETS];
+  uint16_t* dst = ents + (size_t)g * FB_WINDOWS * C;
+  for (uint32_t e = threadIdx.x; e < total; e += blockDim.x) dst[e] = lst[e];
+}
+
+struct FbAccArgs {
+  const G1Aff* tab;     // [cosets][lines][W][N]
+  const uint32_t* offs;
+  const uint16_t* ents;
+  XYZZ* outT;           // [cosets * nchunks * lines][FB_ACC_THREADS]
+  XYZZ* outS;
+  int lr, lc, lines;
+};
+
+// Persistent CTAs over the (chunk, line) work items. Per item:
+//  1. the 1024 buckets are counting-sorted by entry count, and round j gives
+//     thread i the bucket at sorted position 128 j + i, so the 32 lanes of a
+//     warp sum buckets of nearly equal length (no idle lanes);
+//  2. bucket sums go to this CTA's scratch (gbuf, 1024 XYZZ, L2-resident);
+//  3. thread i folds buckets 8i+1 .. 8i+8 into running sums
+//     S_i = sum B_k, T_i = sum (k - 8i) B_k.
+constexpr int FB_COUNT_BINS = 128;  // entry counts >= 127 share the last bin
+__global__ void __launch_bounds__(FB_ACC_THREADS, 4) k_fb_accum(FbAccArgs a, XYZZ* __restrict__ gbuf_all,
+                                                                uint32_t units) {
+  __shared__ uint32_t soffs[FB_BUCKETS + 1];
+  __shared__ uint16_t order[FB_BUCKETS];
+  __shared__ uint32_t bins[FB_COUNT_BINS];
+  XYZZ* gbuf = gbuf_all + (size_t)blockIdx.x * FB_BUCKETS;
+  const uint32_t nch = 1u << a.lr;
+  const uint64_t N = 1ull << (a.lr + a.lc);
+  for (uint32_t u = blockIdx.x; u < units; u += gridDim.x) {
+    const uint32_t l = u % a.lines, g = u / a.lines;
+    const uint32_t coset = g / nch, b = g % nch;
+    const uint32_t* offs = a.offs + (size_t)g * (FB_BUCKETS + 1);
+    const uint16_t* ents = a.ents + (size_t)g * FB_WINDOWS * (1u << a.lc);
+    const G1Aff* tabl = a.tab + ((uint64_t)coset * a.lines + l) * FB_WINDOWS * N + ((uint64_t)b << a.lc);
+    __syncthreads();  // previous item's readers of soffs / order / gbuf are done
+    for (int k = threadIdx.x; k <= FB_BUCKETS; k += blockDim.x) soffs[k] = offs[k];
+    for (int k = threadIdx.x; k < FB_COUNT_BINS; k += blockDim.x) bins[k] = 0;
+    __syncthreads();
+    // bucket k (1-based) has soffs[k] - soffs[k-1] entries; sort descending by count
+    for (int k = threadIdx.x; k < FB_BUCKETS; k += blockDim.x) {
+      uint32_t c = soffs[k + 1] - soffs[k];
+      atomicAdd(&bins[FB_COUNT_BINS - 1 - min(c, (uint32_t)FB_COUNT_BINS - 1)], 1u);
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      uint32_t acc = 0;
+      for (int i = 0; i < FB_COUNT_BINS; ++i) { uint32_t v = bins[i]; bins[i] = acc; acc += v; }
+    }
+    __syncthreads();
+    for (int k = threadIdx.x; k < FB_BUCKETS; k += blockDim.x) {
+      uint32_t c = soffs[k + 1] - soffs[k];
+      uint32_t pos = atomicAdd(&bins[FB_COUNT_BINS - 1 - min(c, (uint32_t)FB_COUNT_BINS - 1)], 1u);
+      order[pos] = (uint16_t)k;  // 0-based bucket index (bucket k + 1)
+    }
+    __syncthreads();
+    for (int r = 0; r < FB_PER_THREAD; ++r) {
+      const uint32_t k = order[r * FB_ACC_THREADS + threadIdx.x];
+      XYZZ B = XYZZ::inf();
+      const uint32_t e1 = soffs[k + 1];
+      for (uint32_t e = soffs[k]; e < e1; ++e) {
+        const uint32_t v = ents[e];
+        G1Aff p = load_aff(tabl + (uint64_t)((v >> 10) & 31) * N + (v & 0x3ff));
+        if (v & 0x8000) p.y = -p.y;
+        B.add_affine(p.x, p.y);
+      }
+      store_xyzz(gbuf + k, B);
+    }
+    __syncthreads();
+    const int k0 = threadIdx.x * FB_PER_THREAD;  // 0-based buckets k0 .. k0+7
+    XYZZ S = XYZZ::inf(), T = XYZZ::inf();
+    for (int k = k0 + FB_PER_THREAD - 1; k >= k0; --k) {
+      S.add(load_xyzz(gbuf + k));
+      T.add(S);
+    }
+    store_xyzz(a.outT + (size_t)u * FB_ACC_THREADS + threadIdx.x, T);
+    store_xyzz(a.outS + (size_t)u * FB_ACC_THREADS + threadIdx.x, S);
+  }
+}
+
+// Per (chunk, line): P = sum_i T_i + 8 * sum_i i S_i; written to
+// part[(coset * lines + l) * nchunks + b] for the AMT trees.
+__global__ void __launch_bounds__(64) k_fb_combine(const XYZZ* __restrict__ T, const XYZZ* __restrict__ S, XYZZ* __restrict__ part,
+                             int lr, int lines, uint32_t count) {
+  const uint32_t u = blockIdx.x * blockDim.x + threadIdx.x;
+  if (u >= count) return;
+  const uint32_t l = u % lines, g = u / lines;
+  const uint32_t nch = 1u << lr;
+  const uint32_t coset = g / nch, b = g % nch;
+  const XYZZ* t = T + (size_t)u * FB_ACC_THREADS;
+  const XYZZ* s = S + (size_t)u * FB_ACC_THREADS;
+  XYZZ tot = XYZZ::inf(), run = XYZZ::inf(), wsum = XYZZ::inf();
+  for (int i = FB_ACC_THREADS - 1; i >= 1; --i) {
+    run.add(load_xyzz(s + i));
+    wsum.add(run);
+  }
+  for (int i = 0; i < FB_ACC_THREADS; ++i) tot.add(load_xyzz(t + i));
+#pragma unroll 1
+  for (int k = 0; k < 3; ++k) wsum = wsum.dbl();  // x FB_PER_THREAD = 8
+  tot.add(wsum);
+  store_xyzz(part + ((size_t)coset * lines + l) * nch + b, tot);
+}
+
 // sum_w 2^{8w} win[w] for each (coset, line, chunk)
-__global__ void k_msm_combine(const XYZZ* __restrict__ win, XYZZ* __restrict__ out, uint32_t count) {
+__global__ void __launch_bounds__(64) k_msm_combine(const XYZZ* __restrict__ win, XYZZ* __restrict__ out, uint32_t count) {
   uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= count) return;
   const XYZZ* w = win + (size_t)i * MSM_WINDOWS;
@@ -363,7 +604,7 @@ __global__ void k_msm_combine(const XYZZ* __restrict__ win, XYZZ* __restrict__ o
 __device__ __forceinline__ uint32_t amt_commit_off(int d) { return 1 + ((2u << d) - 2); }
 __device__ __forceinline__ uint32_t amt_proof_off(int d, int lr) { return (2u << lr) - 1 + ((2u << d) - 2); }
 
-__global__ void k_amt_tree(XYZZ* __restrict__ part, XYZZ* __restrict__ nodes, int lr, int lines) {
+__global__ void __launch_bounds__(256) k_amt_tree(XYZZ* __restrict__ part, XYZZ* __restrict__ nodes, int lr, int lines) {
   const int l = blockIdx.x, c = blockIdx.y;
   const int R = 1 << lr;
   const uint32_t per_coset = 4u * R - 2;
@@ -412,7 +653,7 @@ __global__ void k_amt_tree(XYZZ* __restrict__ part, XYZZ* __restrict__ nodes, in
 }
 
 // XYZZ node -> 64-byte ark G1
-__global__ void k_serialize_nodes(const XYZZ* __restrict__ nodes, uint8_t* __restrict__ out, uint32_t count) {
+__global__ void __launch_bounds__(128) k_serialize_nodes(const XYZZ* __restrict__ nodes, uint8_t* __restrict__ out, uint32_t count) {
   uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= count) return;
   uint8_t buf[64];
@@ -428,7 +669,7 @@ __global__ void k_serialize_nodes(const XYZZ* __restrict__ nodes, uint8_t* __res
 // ---------------------------------------------------------------------------
 // Merkle tree (merkle/blob.rs:15-34): leaves = keccak(8 x 32 B), parents =
 // keccak(left || right) until 3 coset roots remain.
-__global__ void k_merkle_leaves(const uint8_t* __restrict__ data, uint8_t* __restrict__ leaves, uint32_t count) {
+__global__ void __launch_bounds__(128) k_merkle_leaves(const uint8_t* __restrict__ data, uint8_t* __restrict__ leaves, uint32_t count) {
   uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= count) return;
   const uint64_t* src = reinterpret_cast<const uint64_t*>(data + (size_t)i * 256);
@@ -445,7 +686,7 @@ __global__ void k_merkle_leaves(const uint8_t* __restrict__ data, uint8_t* __res
   d[0] = make_ulonglong2(out[0], out[1]);
   d[1] = make_ulonglong2(out[2], out[3]);
 }
-__global__ void k_merkle_parents(const uint8_t* __restrict__ child, uint8_t* __restrict__ parent, uint32_t count) {
+__global__ void __launch_bounds__(128) k_merkle_parents(const uint8_t* __restrict__ child, uint8_t* __restrict__ parent, uint32_t count) {
   uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= count) return;
   const ulonglong2* src = reinterpret_cast<const ulonglong2*>(child + (size_t)i * 64);
@@ -494,7 +735,7 @@ __device__ __forceinline__ void put_u64(uint8_t* p, uint64_t v) {
 #pragma unroll
   for (int i = 0; i < 8; ++i) p[i] = (uint8_t)(v >> (8 * i));
 }
-__global__ void k_slices(SliceArgs a) {
+__global__ void __launch_bounds__(256) k_slices(SliceArgs a) {
   const int R = 1 << a.lr, C = 1 << a.lc;
   const uint32_t index = blockIdx.x;
   const uint32_t coset = index / R, local = index % R;
@@ -568,7 +809,7 @@ __global__ void k_quot_coeff(const Fr* pw, Fr* c, uint32_t M, uint32_t n) {
 
 // generic four-step NTT pass A: for each column s (C of them) of x viewed as
 // [R][C] row-major: R-point transform over q, times w_N^{s r}; writes Y[r][s].
-__global__ void k_ntt4_colpass(const Fr* __restrict__ x, Fr* __restrict__ y, int lr, int lc,
+__global__ void __launch_bounds__(256) k_ntt4_colpass(const Fr* __restrict__ x, Fr* __restrict__ y, int lr, int lc,
                                const Fr* __restrict__ tw_r, const Fr* __restrict__ w_lo,
                                const Fr* __restrict__ w_hi) {
   extern __shared__ __align__(16) uint8_t smem[];
@@ -583,7 +824,7 @@ __global__ void k_ntt4_colpass(const Fr* __restrict__ x, Fr* __restrict__ y, int
     store_fr(y + (size_t)r * C + col, s[r] * pow_split(w_lo, w_hi, col * (uint32_t)r, lc, nmask));
 }
 // pass B: for each r, C-point transform over s of Y[r][*]; out[j R + r]
-__global__ void k_ntt4_rowpass(const Fr* __restrict__ y, Fr* __restrict__ out, int lr, int lc,
+__global__ void __launch_bounds__(256) k_ntt4_rowpass(const Fr* __restrict__ y, Fr* __restrict__ out, int lr, int lc,
                                const Fr* __restrict__ tw_c) {
   extern __shared__ __align__(16) uint8_t smem[];
   const int R = 1 << lr, C = 1 << lc;
@@ -596,7 +837,7 @@ __global__ void k_ntt4_rowpass(const Fr* __restrict__ y, Fr* __restrict__ out, i
 }
 
 // fixed-base table of G: tab[w*255 + d - 1] = d * 2^{8w} * G (XYZZ)
-__global__ void k_fixed_table(XYZZ* tab, G1Aff g) {
+__global__ void __launch_bounds__(32) k_fixed_table(XYZZ* tab, G1Aff g) {
   int w = blockIdx.x * blockDim.x + threadIdx.x;
   if (w >= 32) return;
   XYZZ base = XYZZ::from_affine(g);
@@ -607,7 +848,7 @@ __global__ void k_fixed_table(XYZZ* tab, G1Aff g) {
     acc.add(base);
   }
 }
-__global__ void k_xyzz_to_affine(const XYZZ* in, G1Aff* out, uint32_t n) {
+__global__ void __launch_bounds__(256) k_xyzz_to_affine(const XYZZ* in, G1Aff* out, uint32_t n) {
   uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= n) return;
   G1Aff a;
@@ -615,7 +856,7 @@ __global__ void k_xyzz_to_affine(const XYZZ* in, G1Aff* out, uint32_t n) {
   out[i] = a;
 }
 // out[p] = s[bitrev(p)] * G (enact: normalize + index_reverse, generate.rs:122-126)
-__global__ void k_fixed_mul(const G1Aff* __restrict__ tab, const Fr* __restrict__ sc, G1Aff* __restrict__ out,
+__global__ void __launch_bounds__(256) k_fixed_mul(const G1Aff* __restrict__ tab, const Fr* __restrict__ sc, G1Aff* __restrict__ out,
                             uint32_t n, int logn) {
   uint32_t p = blockIdx.x * blockDim.x + threadIdx.x;
   if (p >= n) return;

@@ -45,6 +45,8 @@ typedef struct zg_config {
   uint64_t tau_seed;       /* params from a seeded tau when params_dir is NULL */
   const char* params_dir;  /* else: amt-prove-coset{0,1,2}-mont-*-{LR:02}-{LR+LC:02}.bin */
   int device;              /* CUDA device ordinal */
+  uint32_t msm_window_bits;/* 0 = auto (11-bit fixed-base windows when the window
+                              tables fit in HBM, else 8-bit), 11, or 8 */
 } zg_config;
 
 /* Builds the device-resident encoder params (3 cosets x (LR + 2) G1 lines).
@@ -83,10 +85,24 @@ typedef struct zg_device_blob {
 } zg_device_blob;
 int zg_encode_device(zg_ctx* ctx, const void* d_data, size_t len, void* stream, zg_device_blob* out);
 
-/* Copy of one device param line (N points, 64 B mont x||y each), the layout
- * of the reference's mont files (fast_serde_bn254.rs:139-160). line < LR:
- * quotients[line]; LR: basis; LR+1: high_basis. */
-int zg_ctx_param_line(zg_ctx* ctx, int coset, int line, uint8_t* host_out, size_t cap);
+/* Copy of points [first, first + count) of one device param line (64 B mont
+ * x||y each), the layout of the reference's mont files
+ * (fast_serde_bn254.rs:139-160). line < LR: quotients[line]; LR: basis;
+ * LR+1: high_basis. */
+int zg_ctx_param_points(zg_ctx* ctx, int coset, int line, size_t first, size_t count, uint8_t* host_out,
+                        size_t cap);
+
+/* Measurement hooks (no reference counterpart; the reference logs tracing
+ * spans, grpc/src/service.rs:68). With profiling on, every encode records CUDA
+ * events between its phases; zg_ctx_phase_times returns the last encode's
+ * phase durations in ms: [RS extension, Merkle, MSM, AMT aggregation,
+ * slice assembly]. zg_ctx_launches counts kernels this context launched. */
+int zg_ctx_set_profiling(zg_ctx* ctx, int enable);
+int zg_ctx_phase_times(zg_ctx* ctx, float* ms, int n);
+uint64_t zg_ctx_launches(const zg_ctx* ctx);
+/* Integer multiply-add rate of the device (independent mad.lo.u32 chains),
+ * in 1e9 per second: the denominator of the MSM roofline. */
+int zg_probe_imad(int device, double* gimad_per_s);
 
 /* Kernel-level entry points (device pointers, stream-ordered on `stream`).
  * zg_msm_chunks: the AMT plugin's MSM decomposition (prove_gpu.rs:55-87):

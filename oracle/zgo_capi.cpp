@@ -404,6 +404,92 @@ int zgo_slice_verify(void* params, const uint8_t* slice, size_t len, const uint8
   return v.code;
 }
 
+
+
+// n pseudo-random G1 points k_i * G (k_i from the SplitMix64 stream at seed),
+// 64 B mont x||y each: stand-in bases for timing samples, where the MSM cost
+// does not depend on which points are summed
+void zgo_random_points(uint64_t seed, size_t n, uint8_t* out) {
+  static FixedBaseG1* fb = nullptr;
+#pragma omp critical(zgo_rand_fb)
+  {
+    if (!fb) fb = new FixedBaseG1(g1_generator());
+  }
+  std::vector<G1J> j(n);
+#pragma omp parallel for schedule(static)
+  for (size_t i = 0; i < n; ++i) j[i] = fb->mul(tau_from_seed(seed + i));
+  std::vector<G1A> a(n);
+  normalize_batch(j.data(), a.data(), n);
+  for (size_t i = 0; i < n; ++i) {
+    memcpy(out + 64 * i, a[i].x.v, 32);
+    memcpy(out + 64 * i + 32, a[i].y.v, 32);
+  }
+}
+
+// ---- CPU baseline ---------------------------------------------------------------
+// Times the restated CPU path on one blob with the MSM work sampled:
+//   t[0] RS extension (RawData -> RawBlob -> 3 cosets, to_coset_blob with
+//        ark-poly style radix-2 transforms) plus Fr -> h256 conversion, full
+//   t[1] keccak Merkle tree, full
+//   t[2] wall time of `S` chunk groups, each the L line-MSMs of one
+//        C-point chunk (the AMT plugin decomposition, prove_gpu.rs:55-87),
+//        run in parallel over all OpenMP threads
+// sample_bases holds, per sampled group, its L lines x C points (mont x||y);
+// sample_chunks[i] = coset * R + chunk.
+int zgo_cpu_baseline(int log_row, int log_col, const uint8_t* data, size_t len, const uint8_t* sample_bases,
+                     const uint32_t* sample_chunks, size_t S, double* t) {
+  Dims d = {log_row, log_col};
+  const size_t N = d.n(), C = d.cols(), R = d.rows();
+  const int L = log_row + 2;
+  double t0 = omp_get_wtime();
+  std::vector<uint8_t> raw;
+  if (!raw_data_from_bytes(d, data, len, &raw)) return -1;
+  std::vector<Fr> blob = raw_blob_from_raw_data(d, raw);
+  std::vector<Fr> points = blob;
+  change_matrix_direction(points, log_col, log_row);
+  std::vector<std::vector<Fr>> cos(COSET_N);
+  for (int c = 0; c < COSET_N; ++c) cos[c] = to_coset_blob(points, c);
+  std::vector<H256> h(COSET_N * N);
+  for (int c = 0; c < COSET_N; ++c) {
+    std::vector<Fr> rm = cos[c];
+    change_matrix_direction(rm, log_row, log_col);
+#pragma omp parallel for schedule(static)
+    for (size_t i = 0; i < N; ++i) h[c * N + i] = scalar_to_h256(rm[i]);
+  }
+  double t1 = omp_get_wtime();
+  Merkle m = merkle_build(d, std::move(h));
+  double t2 = omp_get_wtime();
+  std::vector<std::vector<BigInt>> sc(COSET_N);
+  for (int c = 0; c < COSET_N; ++c) {
+    std::vector<Fr> ri = cos[c];
+    index_reverse(ri);
+    sc[c] = to_bigints(ri.data(), ri.size());
+  }
+  double t3 = omp_get_wtime();
+  std::vector<G1J> out(S * L);
+#pragma omp parallel for schedule(dynamic)
+  for (size_t task = 0; task < S * L; ++task) {
+    size_t gi = task / L, l = task % L;
+    uint32_t cb = sample_chunks[gi];
+    size_t c = cb / R, b = cb % R;
+    std::vector<G1A> bases(C);
+    const uint8_t* src = sample_bases + ((gi * L + l) * C) * 64;
+    for (size_t i = 0; i < C; ++i) {
+      u64 x[4], y[4];
+      memcpy(x, src + 64 * i, 32);
+      memcpy(y, src + 64 * i + 32, 32);
+      bases[i] = {Fq::from_raw_mont(x), Fq::from_raw_mont(y), false};
+    }
+    out[task] = msm(bases.data(), sc[c].data() + b * C, C);
+  }
+  double t4 = omp_get_wtime();
+  t[0] = t1 - t0;
+  t[1] = t2 - t1;
+  t[2] = t4 - t3;
+  (void)m;
+  return 0;
+}
+
 // ---- recovery -----------------------------------------------------------------
 int zgo_recover(int log_row, int log_col, const uint64_t* ids, const uint8_t* const* rows, const size_t* lens,
                 size_t n, uint8_t* out, size_t* out_len, char* msg, size_t msgcap) {

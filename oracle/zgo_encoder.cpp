@@ -115,35 +115,6 @@ static void group_scale(std::vector<Jac<F>>& a, const Fr& s) {
   for (size_t i = 0; i < a.size(); ++i) a[i] = a[i].mul(b);
 }
 
-// fixed-base multiplication table: entry [w][d-1] = d * 2^{8w} * G
-template <class F>
-struct FixedBase {
-  std::vector<Affine<F>> tab;
-  explicit FixedBase(const Affine<F>& g) {
-    std::vector<Jac<F>> j(32 * 255);
-    Jac<F> base = Jac<F>::from_affine(g);
-    for (int w = 0; w < 32; ++w) {
-      Jac<F> acc = base;
-      for (int d = 1; d <= 255; ++d) {
-        j[w * 255 + d - 1] = acc;
-        acc = acc.add(base);
-      }
-      base = acc;  // 256 * base
-    }
-    tab.resize(j.size());
-    normalize_batch(j.data(), tab.data(), j.size());
-  }
-  Jac<F> mul(const Fr& s) const {
-    BigInt k = s.to_bigint();
-    Jac<F> acc = Jac<F>::inf();
-    for (int w = 0; w < 32; ++w) {
-      unsigned d = (k.v[w / 8] >> (8 * (w % 8))) & 0xff;
-      if (d) acc = acc.add_affine(tab[w * 255 + d - 1]);
-    }
-    return acc;
-  }
-};
-
 template <class F>
 static std::vector<Affine<F>> enact(std::vector<Jac<F>>& in) {
   std::vector<Affine<F>> out(in.size());
@@ -517,7 +488,7 @@ std::vector<Fr> to_coset_blob(const std::vector<Fr>& data, size_t coset) {
   return coeff;
 }
 
-static std::vector<BigInt> to_bigints(const Fr* s, size_t n) {
+std::vector<BigInt> to_bigints(const Fr* s, size_t n) {
   std::vector<BigInt> out(n);
   for (size_t i = 0; i < n; ++i) out[i] = s[i].to_bigint();
   return out;

@@ -62,6 +62,37 @@ void fr_ifft(std::vector<Fr>& a);  // inverse, scaled by 1/n
 void fr_ntt_omega(std::vector<Fr>& a, const Fr& omega);
 Fr coset_factor(size_t length, size_t idx);  // prove_params/generate.rs:128-137
 
+// fixed-base multiplication table: entry [w][d-1] = d * 2^{8w} * G
+template <class F>
+struct FixedBase {
+  std::vector<Affine<F>> tab;
+  explicit FixedBase(const Affine<F>& g) {
+    std::vector<Jac<F>> j(32 * 255);
+    Jac<F> base = Jac<F>::from_affine(g);
+    for (int w = 0; w < 32; ++w) {
+      Jac<F> acc = base;
+      for (int d = 1; d <= 255; ++d) {
+        j[w * 255 + d - 1] = acc;
+        acc = acc.add(base);
+      }
+      base = acc;  // 256 * base
+    }
+    tab.resize(j.size());
+    normalize_batch(j.data(), tab.data(), j.size());
+  }
+  Jac<F> mul(const Fr& s) const {
+    BigInt k = s.to_bigint();
+    Jac<F> acc = Jac<F>::inf();
+    for (int w = 0; w < 32; ++w) {
+      unsigned d = (k.v[w / 8] >> (8 * (w % 8))) & 0xff;
+      if (d) acc = acc.add_affine(tab[w * 255 + d - 1]);
+    }
+    return acc;
+  }
+};
+
+typedef FixedBase<Fq> FixedBaseG1;
+
 // ---- params
 struct PowerTau {
   std::vector<G1A> g1pp, high_g1pp;
@@ -140,6 +171,7 @@ struct EncodedBlob {
 bool raw_data_from_bytes(const Dims& d, const uint8_t* in, size_t len, std::vector<uint8_t>* out);
 std::vector<Fr> raw_blob_from_raw_data(const Dims& d, const std::vector<uint8_t>& raw);
 std::vector<Fr> to_coset_blob(const std::vector<Fr>& data, size_t coset);
+std::vector<BigInt> to_bigints(const Fr* s, size_t n);
 AllProofs gen_all_proofs(const AMTParams& amt, const std::vector<Fr>& ri_data, G1J* commitment);
 HalfBlob half_blob_generate(const Dims& d, std::vector<Fr> points, const AMTParams& amt);
 Merkle merkle_build(const Dims& d, std::vector<H256> data);

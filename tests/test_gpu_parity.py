@@ -185,6 +185,42 @@ def test_encode_matches_oracle(gpu_pkg, oracle, log_row, log_col):
     params.close()
 
 
+@pytest.mark.parametrize("bits", [8, 11])
+def test_encode_msm_variants_match_oracle(gpu_pkg, oracle, bits):
+    """Both MSM variants (8-bit windows with doublings; 11-bit fixed-base
+    window tables) give the oracle's bytes."""
+    params = gpu_pkg.ZgEncoderParams.from_seed(5, 6, 31, msm_window_bits=bits)
+    op = oracle.params(5, 6, 31)
+    payload = np.random.default_rng(bits).integers(0, 256, size=params.dims.max_raw_data_size - 7,
+                                                   dtype=np.uint8).tobytes()
+    _check_against_oracle(gpu_pkg, oracle, params, op, payload)
+    params.close()
+
+
+def test_device_encode_then_host_encode_are_ordered(gpu_pkg, oracle):
+    """zg_encode_device on a caller stream followed at once by zg_encode on the
+    context stream: both share the context scratch and must not overlap."""
+    torch = torch_mod()
+    params = gpu_pkg.ZgEncoderParams.from_seed(4, 6, 77)
+    op = oracle.params(4, 6, 77)
+    L = gpu_pkg.lib()
+    rng = np.random.default_rng(9)
+    a = rng.integers(0, 256, size=5000, dtype=np.uint8).tobytes()
+    b = rng.integers(0, 256, size=3000, dtype=np.uint8).tobytes()
+    s = torch.cuda.Stream()
+    ta = dev(a)
+    db = gpu_pkg._DeviceBlob()
+    for _ in range(3):
+        rc = L.zg_encode_device(params.handle, ctypes.c_void_p(ta.data_ptr()), len(a),
+                                ctypes.c_void_p(s.cuda_stream), ctypes.byref(db))
+        assert rc == 0
+    reply = gpu_pkg.EncoderService(params).process_data(b, True)
+    ob = oracle.encode(op, b)
+    assert reply.encoded_data == ob.data()
+    assert reply.encoded_slice[5] == ob.slice(5)
+    params.close()
+
+
 def test_encode_zero_blob_is_infinity(gpu_pkg, oracle):
     """An empty payload encodes to the all-zero blob: every commitment and
     proof is the point at infinity (ark flag bit 6)."""

@@ -46,6 +46,9 @@ _SIGS = {
                                         ctypes.POINTER(ctypes.c_int64)]),
     "zgo_merkle_roots": (None, [ctypes.c_int, ctypes.c_int, ctypes.c_char_p, ctypes.c_char_p]),
     "zgo_verify_params_new": (_P, [ctypes.c_int, ctypes.c_int, ctypes.c_uint64, ctypes.c_char_p]),
+    "zgo_cpu_baseline": (ctypes.c_int, [ctypes.c_int, ctypes.c_int, ctypes.c_char_p, _SZ, ctypes.c_char_p,
+                                        ctypes.POINTER(ctypes.c_uint32), _SZ, ctypes.POINTER(ctypes.c_double)]),
+    "zgo_random_points": (None, [ctypes.c_uint64, _SZ, ctypes.c_char_p]),
     "zgo_recover": (ctypes.c_int, [ctypes.c_int, ctypes.c_int, ctypes.POINTER(ctypes.c_uint64),
                                    ctypes.POINTER(ctypes.c_char_p), ctypes.POINTER(_SZ), _SZ,
                                    ctypes.c_char_p, ctypes.POINTER(_SZ), ctypes.c_char_p, _SZ]),
@@ -244,6 +247,20 @@ class Oracle:
         n = self.L.zgo_amt_scalar_domain(log_row, log_col, seed, coset, coset_rows, out)
         assert n == 4 * R - 2
         return out.raw
+
+    def random_points(self, seed, n):
+        out = ctypes.create_string_buffer(64 * n)
+        self.L.zgo_random_points(seed, n, out)
+        return out.raw
+
+    def cpu_baseline(self, log_row, log_col, data: bytes, sample_bases: bytes, sample_chunks):
+        """(rs_s, merkle_s, msm_sample_s) of the restated CPU path; see oracle/zgo_capi.cpp."""
+        S = len(sample_chunks)
+        arr = (ctypes.c_uint32 * S)(*sample_chunks)
+        t = (ctypes.c_double * 3)()
+        rc = self.L.zgo_cpu_baseline(log_row, log_col, data, len(data), sample_bases, arr, S, t)
+        assert rc == 0
+        return tuple(t)
 
     def recover(self, log_row, log_col, rows: dict):
         ids = sorted(rows)
