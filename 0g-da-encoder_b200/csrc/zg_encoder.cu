@@ -203,7 +203,7 @@ struct zg_ctx {
   uint16_t* fb_ents = nullptr;
   XYZZ* fb_T = nullptr;
   XYZZ* fb_S = nullptr;
-  XYZZ* fb_gbuf = nullptr;  // per persistent CTA bucket sums
+  XYZZ* fb_gbuf = nullptr;  // per persistent CTA task partial sums
   unsigned fb_ctas = 0;
   uint8_t* raw = nullptr;
   uint8_t* enc = nullptr;
@@ -256,7 +256,7 @@ int alloc_blob_buffers(zg_ctx* c) {
     ZG_CK(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, c->device));
     ZG_CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_fb_accum, FB_ACC_THREADS, 0));
     c->fb_ctas = (unsigned)std::max(1, sms * std::max(1, per_sm));
-    ZG_CK(cudaMalloc(&c->fb_gbuf, (size_t)c->fb_ctas * FB_BUCKETS * sizeof(XYZZ)));
+    ZG_CK(cudaMalloc(&c->fb_gbuf, (size_t)c->fb_ctas * FB_MAX_TASKS * sizeof(XYZZ)));
   }
   ZG_CK(cudaMalloc(&c->raw, c->max_blob + 16));
   ZG_CK(cudaMalloc(&c->enc, 3 * N * 32));

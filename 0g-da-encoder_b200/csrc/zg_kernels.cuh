@@ -493,19 +493,24 @@ struct FbAccArgs {
 };
 
 // Persistent CTAs over the (chunk, line) work items. Per item:
-//  1. the 1024 buckets are counting-sorted by entry count, and round j gives
-//     thread i the bucket at sorted position 128 j + i, so the 32 lanes of a
-//     warp sum buckets of nearly equal length (no idle lanes);
-//  2. bucket sums go to this CTA's scratch (gbuf, 1024 XYZZ, L2-resident);
-//  3. thread i folds buckets 8i+1 .. 8i+8 into running sums
-//     S_i = sum B_k, T_i = sum (k - 8i) B_k.
-constexpr int FB_COUNT_BINS = 128;  // entry counts >= 127 share the last bin
-__global__ void __launch_bounds__(FB_ACC_THREADS, 4) k_fb_accum(FbAccArgs a, XYZZ* __restrict__ gbuf_all,
+//  1. every bucket is cut into tasks of at most FB_TASK entries (the top
+//     window's digits are tiny, so buckets 1 and 2 hold ~10x the average);
+//  2. tasks are counting-sorted by size and round r gives thread i the task at
+//     sorted position 128 r + i: the 32 lanes of a warp run tasks of nearly
+//     equal length;
+//  3. task partial sums go to this CTA's scratch (gpart, L2-resident);
+//  4. thread i merges the partials of buckets 8i+1 .. 8i+8 and folds them
+//     into running sums S_i = sum B_k, T_i = sum (k - 8i) B_k.
+constexpr int FB_TASK = 32;
+constexpr int FB_MAX_TASKS = FB_BUCKETS + FB_WINDOWS * 1024 / FB_TASK;  // chunk <= 1024 points
+__global__ void __launch_bounds__(FB_ACC_THREADS, 4) k_fb_accum(FbAccArgs a, XYZZ* __restrict__ gpart_all,
                                                                 uint32_t units) {
   __shared__ uint32_t soffs[FB_BUCKETS + 1];
-  __shared__ uint16_t order[FB_BUCKETS];
-  __shared__ uint32_t bins[FB_COUNT_BINS];
-  XYZZ* gbuf = gbuf_all + (size_t)blockIdx.x * FB_BUCKETS;
+  __shared__ uint16_t tstart[FB_BUCKETS + 1];
+  __shared__ uint16_t order[FB_MAX_TASKS];
+  __shared__ uint16_t tbucket[FB_MAX_TASKS];
+  __shared__ uint32_t bins[FB_TASK + 1];
+  XYZZ* gpart = gpart_all + (size_t)blockIdx.x * FB_MAX_TASKS;
   const uint32_t nch = 1u << a.lr;
   const uint64_t N = 1ull << (a.lr + a.lc);
   for (uint32_t u = blockIdx.x; u < units; u += gridDim.x) {
@@ -514,44 +519,79 @@ __global__ void __launch_bounds__(FB_ACC_THREADS, 4) k_fb_accum(FbAccArgs a, XYZ
     const uint32_t* offs = a.offs + (size_t)g * (FB_BUCKETS + 1);
     const uint16_t* ents = a.ents + (size_t)g * FB_WINDOWS * (1u << a.lc);
     const G1Aff* tabl = a.tab + ((uint64_t)coset * a.lines + l) * FB_WINDOWS * N + ((uint64_t)b << a.lc);
-    __syncthreads();  // previous item's readers of soffs / order / gbuf are done
+    __syncthreads();  // the previous item is finished with the shared arrays and gpart
     for (int k = threadIdx.x; k <= FB_BUCKETS; k += blockDim.x) soffs[k] = offs[k];
-    for (int k = threadIdx.x; k < FB_COUNT_BINS; k += blockDim.x) bins[k] = 0;
+    for (int k = threadIdx.x; k <= FB_TASK; k += blockDim.x) bins[k] = 0;
     __syncthreads();
-    // bucket k (1-based) has soffs[k] - soffs[k-1] entries; sort descending by count
+    // tasks per bucket, exclusive scan -> tstart (bucket k = 0-based index)
+    if (threadIdx.x < 32) {
+      // warp-level scan over 1024 buckets, 32 per lane
+      const int lane = threadIdx.x;
+      uint32_t loc[32];
+      uint32_t sum = 0;
+      for (int i = 0; i < 32; ++i) {
+        const int k = lane * 32 + i;
+        const uint32_t c = soffs[k + 1] - soffs[k];
+        loc[i] = (c + FB_TASK - 1) / FB_TASK;
+        sum += loc[i];
+      }
+      uint32_t incl = sum;
+      for (int d = 1; d < 32; d <<= 1) {
+        uint32_t v = __shfl_up_sync(0xffffffffu, incl, d);
+        if (lane >= d) incl += v;
+      }
+      uint32_t acc = incl - sum;
+      for (int i = 0; i < 32; ++i) {
+        tstart[lane * 32 + i] = (uint16_t)acc;
+        acc += loc[i];
+      }
+      if (lane == 31) tstart[FB_BUCKETS] = (uint16_t)acc;
+    }
+    __syncthreads();
+    const uint32_t ntasks = tstart[FB_BUCKETS];
+    // size of task j of bucket k: FB_TASK except the bucket's last task
     for (int k = threadIdx.x; k < FB_BUCKETS; k += blockDim.x) {
-      uint32_t c = soffs[k + 1] - soffs[k];
-      atomicAdd(&bins[FB_COUNT_BINS - 1 - min(c, (uint32_t)FB_COUNT_BINS - 1)], 1u);
+      const uint32_t c = soffs[k + 1] - soffs[k];
+      for (uint32_t t = tstart[k]; t < tstart[k + 1]; ++t) {
+        tbucket[t] = (uint16_t)k;
+        const uint32_t j = t - tstart[k];
+        const uint32_t sz = min((uint32_t)FB_TASK, c - j * FB_TASK);
+        atomicAdd(&bins[FB_TASK - sz], 1u);
+      }
     }
     __syncthreads();
     if (threadIdx.x == 0) {
       uint32_t acc = 0;
-      for (int i = 0; i < FB_COUNT_BINS; ++i) { uint32_t v = bins[i]; bins[i] = acc; acc += v; }
+      for (int i = 0; i <= FB_TASK; ++i) { uint32_t v = bins[i]; bins[i] = acc; acc += v; }
     }
     __syncthreads();
-    for (int k = threadIdx.x; k < FB_BUCKETS; k += blockDim.x) {
-      uint32_t c = soffs[k + 1] - soffs[k];
-      uint32_t pos = atomicAdd(&bins[FB_COUNT_BINS - 1 - min(c, (uint32_t)FB_COUNT_BINS - 1)], 1u);
-      order[pos] = (uint16_t)k;  // 0-based bucket index (bucket k + 1)
+    for (uint32_t t = threadIdx.x; t < ntasks; t += blockDim.x) {
+      const uint32_t k = tbucket[t];
+      const uint32_t c = soffs[k + 1] - soffs[k];
+      const uint32_t j = t - tstart[k];
+      const uint32_t sz = min((uint32_t)FB_TASK, c - j * FB_TASK);
+      order[atomicAdd(&bins[FB_TASK - sz], 1u)] = (uint16_t)t;
     }
     __syncthreads();
-    for (int r = 0; r < FB_PER_THREAD; ++r) {
-      const uint32_t k = order[r * FB_ACC_THREADS + threadIdx.x];
+    for (uint32_t r = threadIdx.x; r < ntasks; r += blockDim.x) {
+      const uint32_t t = order[r];
+      const uint32_t k = tbucket[t];
+      const uint32_t e0 = soffs[k] + (t - tstart[k]) * FB_TASK;
+      const uint32_t e1 = min(e0 + FB_TASK, soffs[k + 1]);
       XYZZ B = XYZZ::inf();
-      const uint32_t e1 = soffs[k + 1];
-      for (uint32_t e = soffs[k]; e < e1; ++e) {
+      for (uint32_t e = e0; e < e1; ++e) {
         const uint32_t v = ents[e];
         G1Aff p = load_aff(tabl + (uint64_t)((v >> 10) & 31) * N + (v & 0x3ff));
         if (v & 0x8000) p.y = -p.y;
         B.add_affine(p.x, p.y);
       }
-      store_xyzz(gbuf + k, B);
+      store_xyzz(gpart + t, B);
     }
     __syncthreads();
     const int k0 = threadIdx.x * FB_PER_THREAD;  // 0-based buckets k0 .. k0+7
     XYZZ S = XYZZ::inf(), T = XYZZ::inf();
     for (int k = k0 + FB_PER_THREAD - 1; k >= k0; --k) {
-      S.add(load_xyzz(gbuf + k));
+      for (uint32_t t = tstart[k]; t < tstart[k + 1]; ++t) S.add(load_xyzz(gpart + t));
       T.add(S);
     }
     store_xyzz(a.outT + (size_t)u * FB_ACC_THREADS + threadIdx.x, T);
