@@ -82,6 +82,7 @@ _SIGS = {
     "zg_ctx_launches": (ctypes.c_uint64, [_P]),
     "zg_probe_imad": (ctypes.c_int, [ctypes.c_int, ctypes.POINTER(ctypes.c_double)]),
     "zg_msm_chunks": (ctypes.c_int, [_P, _P, ctypes.c_uint32, ctypes.c_uint32, ctypes.c_uint32, _P, _P]),
+    "zg_msm_chunks_noalloc": (ctypes.c_int, [_P, _P, ctypes.c_uint32, ctypes.c_uint32, ctypes.c_uint32, _P, _P]),
     "zg_ntt": (ctypes.c_int, [_P, ctypes.c_uint32, ctypes.c_uint32, ctypes.c_int, ctypes.c_uint32, _P]),
     "zg_merkle_roots": (ctypes.c_int, [_P, _SZ, _P, _P]),
     "zg_selftest": (ctypes.c_int, [ctypes.POINTER(ctypes.c_int), ctypes.c_int]),

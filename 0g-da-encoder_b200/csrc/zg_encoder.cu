@@ -186,6 +186,14 @@ void ntt4(const Twiddles& tw, const Fr* x, Fr* tmp, Fr* out, bool inverse, cudaS
 
 }  // namespace
 
+// Scratch of zg_msm_chunks_noalloc: window sums and per-MSM results of at
+// most ZG_NOALLOC_MAX_MSMS chunk MSMs (lines x chunks). It lives in the
+// module's static device memory, so every GPU that loads this library holds
+// these ~4.3 MB until the process exits.
+constexpr uint32_t ZG_NOALLOC_MAX_MSMS = 1024;
+static __device__ __align__(256) uint8_t g_noalloc_scratch[(size_t)ZG_NOALLOC_MAX_MSMS * (MSM_WINDOWS + 1) *
+                                                           sizeof(XYZZ)];
+
 struct zg_ctx {
   int device = 0;
   int lr = 0, lc = 0, L = 0;
@@ -840,6 +848,61 @@ int zg_msm_chunks(const void* d_bases, const void* d_scalars, uint32_t lines, ui
   cudaFreeAsync(win, s);
   cudaFreeAsync(part, s);
   return rc;
+}
+
+// Allocation-free twin of zg_msm_chunks: same kernels, with the scratch in
+// g_noalloc_scratch. Host code must not hand the array's name to a kernel (on
+// the host it names a stand-in, not device memory), so its device address is
+// looked up with cudaGetSymbolAddress once per device, with that device
+// current, on the first call made on it; later calls reuse the cached address.
+int zg_msm_chunks_noalloc(const void* d_bases, const void* d_scalars, uint32_t lines, uint32_t log_nchunks,
+                          uint32_t log_chunk, void* d_out, void* stream) {
+  static std::mutex mu;
+  static void* addr[256] = {nullptr};
+  if (!d_bases || !d_scalars || !d_out || lines == 0 || log_chunk > 10 || log_nchunks > 20)
+    return fail(ZG_ERR_INVALID_ARG, "bad msm arguments");
+  const uint64_t count = (uint64_t)lines << log_nchunks;
+  if (count > ZG_NOALLOC_MAX_MSMS) {
+    char m[160];
+    snprintf(m, sizeof(m), "zg_msm_chunks_noalloc: lines * 2^log_nchunks = %llu exceeds the static scratch limit %u",
+             (unsigned long long)count, ZG_NOALLOC_MAX_MSMS);
+    return fail(ZG_ERR_INVALID_ARG, m);
+  }
+  int dev = 0;
+  ZG_CK(cudaGetDevice(&dev));
+  if (dev < 0 || dev >= 256) return fail(ZG_ERR_INVALID_ARG, "device ordinal out of range");
+  void* scratch = nullptr;
+  {
+    std::lock_guard<std::mutex> g(mu);
+    if (!addr[dev]) {
+      cudaError_t e = cudaGetSymbolAddress(&addr[dev], g_noalloc_scratch);
+      if (e != cudaSuccess) {
+        addr[dev] = nullptr;
+        return fail(ZG_ERR_CUDA, std::string("cudaGetSymbolAddress(g_noalloc_scratch): ") + cudaGetErrorString(e));
+      }
+    }
+    scratch = addr[dev];
+  }
+  int rc = set_smem_limits();
+  if (rc) return rc;
+  cudaStream_t s = (cudaStream_t)stream;
+  XYZZ* win = reinterpret_cast<XYZZ*>(scratch);
+  XYZZ* part = win + count * MSM_WINDOWS;
+  MsmChunkArgs a;
+  a.scalars = (const uint8_t*)d_scalars;
+  a.bases = (const G1Aff*)d_bases;
+  a.win = win;
+  a.lr = (int)log_nchunks;
+  a.lc = (int)log_chunk;
+  a.lines = (int)lines;
+  a.bitrev_rows = 0;
+  a.scalar_coset_stride = 0;
+  a.base_coset_stride = 0;
+  a.base_line_stride = (uint64_t)1 << (log_nchunks + log_chunk);
+  k_msm_chunks<<<dim3(1u << log_nchunks, 1), MSM_THREADS, msm_smem_bytes((int)log_chunk), s>>>(a);
+  k_msm_combine<<<nblk(count, 64), 64, 0, s>>>(win, part, (uint32_t)count);
+  k_serialize_nodes<<<nblk(count, 128), 128, 0, s>>>(part, (uint8_t*)d_out, (uint32_t)count);
+  return check_launch();
 }
 
 int zg_ntt(void* d_data, uint32_t log_n, uint32_t batch, int inverse, uint32_t coset_idx, void* stream) {

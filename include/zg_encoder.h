@@ -112,6 +112,22 @@ int zg_probe_imad(int device, double* gimad_per_s);
  * nchunks and chunk are powers of two, chunk <= 1024. */
 int zg_msm_chunks(const void* d_bases, const void* d_scalars, uint32_t lines, uint32_t log_nchunks,
                   uint32_t log_chunk, void* d_out, void* stream);
+/* Allocation-free variant of zg_msm_chunks (no counterpart in the reference).
+ * Same arguments and results, but it calls no cudaMalloc / cudaFree and no
+ * allocating library routine: its scratch is a static device array sized for
+ * at most 1024 chunk MSMs (lines * 2^log_nchunks <= 1024; larger requests
+ * fail with ZG_ERR_INVALID_ARG). It is meant for callers that cannot
+ * allocate device memory per call, such as a process that has handed all
+ * free HBM to another allocator at start-up, or a loop that must never block
+ * on cudaMalloc (which can synchronize the device).
+ * The first call on a device looks the array's device address up
+ * (cudaGetSymbolAddress) with that device current; make that first call
+ * before any stream capture. Every call on a device shares the one array
+ * (it keeps the last call's contents; every element is written before it is
+ * read, so nothing needs clearing), so calls that overlap on the GPU, e.g. on
+ * two streams at once, race: order them on one stream or with events. */
+int zg_msm_chunks_noalloc(const void* d_bases, const void* d_scalars, uint32_t lines, uint32_t log_nchunks,
+                          uint32_t log_chunk, void* d_out, void* stream);
 /* Batched radix-2 NTT over Fr with ark-poly Radix2EvaluationDomain semantics
  * (crates/amt/src/blob/encode.rs:142-157): `batch` contiguous vectors of
  * 2^log_n canonical 32-byte elements, transformed in place. inverse != 0
