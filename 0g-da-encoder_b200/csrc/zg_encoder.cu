@@ -240,6 +240,34 @@ struct zg_ctx {
   std::mutex mu;
 };
 
+// Process-wide pool of page-locked reply buffers: pinning ~200 MB per reply
+// costs far more than the copies themselves, so freed buffers are kept (a few
+// per size) for the next reply.
+namespace {
+std::mutex g_pin_mu;
+std::multimap<size_t, void*> g_pin_pool;
+void* pinned_get(size_t bytes) {
+  {
+    std::lock_guard<std::mutex> g(g_pin_mu);
+    auto it = g_pin_pool.find(bytes);
+    if (it != g_pin_pool.end()) {
+      void* p = it->second;
+      g_pin_pool.erase(it);
+      return p;
+    }
+  }
+  void* p = nullptr;
+  if (cudaMallocHost(&p, bytes) != cudaSuccess) return nullptr;
+  return p;
+}
+void pinned_put(void* p, size_t bytes) {
+  if (!p) return;
+  std::lock_guard<std::mutex> g(g_pin_mu);
+  if (g_pin_pool.count(bytes) < 4) g_pin_pool.emplace(bytes, p);
+  else cudaFreeHost(p);
+}
+}  // namespace
+
 struct zg_reply {
   uint32_t version = 0;
   uint8_t commitment[64];
@@ -697,11 +725,11 @@ int zg_encode(zg_ctx* c, const uint8_t* data, size_t len, int require_data, zg_r
   };
   r->slice_size = c->slice_size;
   r->nslices = 3 * c->R;
-  if (cudaMallocHost(&r->slices, r->nslices * r->slice_size) != cudaSuccess)
+  if (!(r->slices = (uint8_t*)pinned_get(r->nslices * r->slice_size)))
     return bail(fail(ZG_ERR_CUDA, "cannot allocate pinned reply"));
   if (require_data) {
     r->data_len = 3 * c->N * 32;
-    if (cudaMallocHost(&r->data, r->data_len) != cudaSuccess)
+    if (!(r->data = (uint8_t*)pinned_get(r->data_len)))
       return bail(fail(ZG_ERR_CUDA, "cannot allocate pinned reply"));
   }
   // page-locked caller buffers are copied by DMA directly; pageable ones go
@@ -754,8 +782,8 @@ int zg_ctx_warmup(zg_ctx* c) {
 
 void zg_reply_free(zg_reply* r) {
   if (!r) return;
-  if (r->slices) cudaFreeHost(r->slices);
-  if (r->data) cudaFreeHost(r->data);
+  pinned_put(r->slices, r->nslices * r->slice_size);
+  pinned_put(r->data, r->data_len);
   delete r;
 }
 uint32_t zg_reply_version(const zg_reply* r) { return r->version; }

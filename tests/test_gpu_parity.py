@@ -343,3 +343,19 @@ def test_production_slices_verify(prod, oracle):
     for i in [0, 1023, 1024, 3071] + rnd.sample(range(3072), 4):
         rc, det = oracle.verify(vp, reply.encoded_slice[i], reply.erasure_commitment, reply.storage_root)
         assert rc == zgo.V_OK, (i, rc, det)
+
+
+def test_encode_matches_golden_fixture(gpu_pkg):
+    """The CUDA path against the independent pure-Python restatement's bytes
+    (tests/golden/make_golden.py, 8 x 32 blob)."""
+    import hashlib
+    import json
+    import os
+    g = json.load(open(os.path.join(os.path.dirname(__file__), "golden", "encode_3x5.json")))["encode"]
+    params = gpu_pkg.ZgEncoderParams.from_seed(g["log_row"], g["log_col"], g["seed"])
+    reply = gpu_pkg.EncoderService(params).process_data(bytes.fromhex(g["payload_hex"]), True)
+    assert reply.erasure_commitment.hex() == g["erasure_commitment"]
+    assert reply.storage_root.hex() == g["file_root"]
+    assert hashlib.sha256(reply.encoded_data).hexdigest() == g["encoded_data_sha256"]
+    assert [hashlib.sha256(s).hexdigest() for s in reply.encoded_slice] == g["slice_sha256"]
+    params.close()

@@ -1,0 +1,282 @@
+"""CPU tests of the oracle (the checker): pinned against an independent pure-
+Python restatement (tests/golden/), Python big integers, hashlib's SHA3
+permutation, and the relations the reference's own tests check."""
+import hashlib
+import json
+import os
+import random
+import sys
+
+import numpy as np
+import pytest
+
+import zgo
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, os.path.join(HERE, "golden"))
+import make_golden as mg  # noqa: E402
+
+R_MOD, Q_MOD = zgo.R_MOD, zgo.Q_MOD
+GOLDEN = json.load(open(os.path.join(HERE, "golden", "encode_3x5.json")))
+
+
+def fr_bytes(vals):
+    return b"".join(v.to_bytes(32, "little") for v in vals)
+
+
+def fr_vals(buf):
+    return [int.from_bytes(buf[32 * i:32 * i + 32], "little") for i in range(len(buf) // 32)]
+
+
+# ---- pins --------------------------------------------------------------------
+def test_keccak_permutation_matches_sha3(oracle):
+    rng = random.Random(1)
+    for n in (0, 1, 31, 32, 64, 135, 136, 137, 256, 300):
+        m = bytes(rng.randrange(256) for _ in range(n))
+        assert oracle.keccak256(m, pad=0x06) == hashlib.sha3_256(m).digest()
+
+
+def test_golden_vectors(oracle):
+    v = GOLDEN["vectors"]
+    for m, h in v["keccak256"].items():
+        assert oracle.keccak256(bytes.fromhex(m)).hex() == h
+    for k, s in v["g1_mul"].items():
+        assert oracle.g1_mul_gen(int(k, 16)).hex() == s
+    assert v["coset_factor_16_1_eq_root_32"]
+    assert oracle.root_of_unity(28) == int(v["root_of_unity_28"], 16)
+
+
+def test_golden_encode_3x5(oracle):
+    """Byte parity with the pure-Python restatement (tests/golden/make_golden.py)."""
+    e = GOLDEN["encode"]
+    op = oracle.params(e["log_row"], e["log_col"], e["seed"])
+    ob = oracle.encode(op, bytes.fromhex(e["payload_hex"]))
+    assert hex(oracle.tau(e["seed"])) == e["tau"]
+    assert ob.commitment().hex() == e["erasure_commitment"]
+    assert [ob.roots()[32 * i:32 * i + 32].hex() for i in range(3)] == e["roots"]
+    assert ob.file_root().hex() == e["file_root"]
+    assert hashlib.sha256(ob.data()).hexdigest() == e["encoded_data_sha256"]
+    for i, h in enumerate(e["slice_sha256"]):
+        s = ob.slice(i)
+        assert len(s) == e["slice_size"]
+        assert hashlib.sha256(s).hexdigest() == h, i
+
+
+def test_fr_mul_matches_python(oracle):
+    import ctypes
+    rng = random.Random(2)
+    out = ctypes.create_string_buffer(32)
+    for _ in range(200):
+        a, b = rng.randrange(R_MOD), rng.randrange(R_MOD)
+        oracle.L.zgo_fr_mul(a.to_bytes(32, "little"), b.to_bytes(32, "little"), out)
+        assert int.from_bytes(out.raw, "little") == a * b % R_MOD
+
+
+@pytest.mark.parametrize("log_n", [1, 2, 4, 6])
+def test_ntt_matches_naive_dft(oracle, log_n):
+    rng = random.Random(log_n)
+    n = 1 << log_n
+    v = [rng.randrange(R_MOD) for _ in range(n)]
+    w = pow(5, (R_MOD - 1) >> log_n, R_MOD)
+    assert fr_vals(oracle.ntt(fr_bytes(v))) == mg.dft(v, w)
+    assert fr_vals(oracle.ntt(oracle.ntt(fr_bytes(v)), inverse=True)) == v
+    # coset: coefficient i scaled by coset_factor(n, 1)^i before the transform
+    g = oracle.coset_factor(n, 1)
+    assert fr_vals(oracle.ntt(fr_bytes(v), coset_idx=1, coset_len=n)) == \
+        mg.dft([x * pow(g, i, R_MOD) % R_MOD for i, x in enumerate(v)], w)
+
+
+def test_coset_factor(oracle):
+    """test_coset_factor (crates/amt/src/blob/encode.rs:349-355) and the
+    production cosets g1 = w_{2^21}, g2 = w_{2^22}."""
+    assert oracle.coset_factor(16, 1) == oracle.root_of_unity(5)
+    assert oracle.coset_factor(1 << 20, 1) == oracle.root_of_unity(21)
+    assert oracle.coset_factor(1 << 20, 2) == oracle.root_of_unity(22)
+    assert oracle.coset_factor(1 << 20, 3) == pow(oracle.root_of_unity(22), 3, R_MOD)
+
+
+def test_pairing_bilinear(oracle):
+    for seed in (3, 11):
+        assert oracle.L.zgo_pairing_selftest(seed) == 1
+
+
+def test_params_ec_domain_equals_scalar_domain(oracle):
+    """AMTParams::from_pp restated with G1/G2 FFTs (generate.rs:139-263)
+    equals the scalar-domain builder, mont file bytes included."""
+    ec = oracle.params(3, 5, 42, ec_domain=True)
+    sd = oracle.params(3, 5, 42)
+    for c in range(3):
+        assert ec.mont(c) == sd.mont(c)
+
+
+def test_erasure_encoding(oracle):
+    """test_erasure_encoding (crates/amt/src/blob/encode.rs:316-347): coset 0
+    and coset 1 are the even / odd samples of the 2N-point transform of the
+    data polynomial."""
+    lr, lc = 3, 5
+    n = 1 << (lr + lc)
+    op = oracle.params(lr, lc, 5)
+    payload = bytes(random.Random(5).randrange(256) for _ in range(7000))
+    data = oracle.encode(op, payload).data()
+    rows = lambda c: fr_vals(data[c * n * 32:(c + 1) * n * 32])
+    col_major = lambda v: [v[r * (1 << lc) + j] for j in range(1 << lc) for r in range(1 << lr)]
+    pts = col_major(rows(0))
+    coeff = fr_vals(oracle.ntt(fr_bytes(pts), inverse=True))
+    big = fr_vals(oracle.ntt(fr_bytes(coeff + [0] * n)))
+    assert col_major(rows(0)) == big[0::2]
+    assert col_major(rows(1)) == big[1::2]
+
+
+# ---- verify and the reference's fault-injection table ------------------------
+def slice_layout(lr, lc):
+    C = 1 << lc
+    a = 96 + 32 * C
+    h = a + 8 + 128 * lr
+    m = h + 64
+    t = m + 104 + 32 * lr
+    return {"row": 96, "proof": a + 8, "high": h, "merkle": m, "mproof": m + 104, "leaf_index": t,
+            "leaf": t + 8, "end": t + 40}
+
+
+def parse_g1(b):
+    if b[63] & 0x40:
+        return None
+    y = bytearray(b[32:])
+    y[31] &= 0x3F
+    return int.from_bytes(b[:32], "little"), int.from_bytes(bytes(y), "little")
+
+
+def bump(h):  # H256::from_low_u64_be(H256(h).to_low_u64_be() + 1)
+    return bytes(24) + ((int.from_bytes(h[24:], "big") + 1) & ((1 << 64) - 1)).to_bytes(8, "big")
+
+
+@pytest.fixture(scope="module")
+def blob_4x6(oracle):
+    op = oracle.params(4, 6, 99)
+    payload = bytes(random.Random(222).randrange(256) for _ in range(1234))
+    ob = oracle.encode(op, payload)
+    return op, ob, [ob.slice(i) for i in range(48)]
+
+
+def test_every_slice_verifies(oracle, blob_4x6):
+    """test_batcher_and_verify (crates/encoder/src/encoder/blob.rs:282-293)."""
+    op, ob, slices = blob_4x6
+    for i, s in enumerate(slices):
+        rc, det = oracle.verify(op, s, ob.commitment(), ob.file_root())
+        assert rc == zgo.V_OK, (i, rc, det)
+
+
+@pytest.mark.parametrize("index", [0, 1, 15, 16, 37, 47])
+def test_fault_injection_error_codes(oracle, blob_4x6, index):
+    """gen_err_signer_map / get_invalid_row (crates/encoder/src/encoder/blob.rs:84-229,
+    amt/blob.rs:61-96, merkle/blob.rs:60-106): each corruption yields exactly
+    the reference's VerifierError variant."""
+    op, ob, slices = blob_4x6
+    R = 16
+    lay = slice_layout(4, 6)
+    s = slices[index]
+    coset, local = divmod(index, R)
+    com, root = ob.commitment(), ob.file_root()
+
+    def check(buf, code, sub=0, a=0, b=0, c=0):
+        rc, det = oracle.verify(op, bytes(buf), com, root)
+        assert rc == code, (index, rc, det)
+        if code in (zgo.V_AMT_INCORRECT_PROOF,):
+            assert det[0] == sub
+        assert det[1:] == [a, b, c], (index, rc, det)
+
+    u64 = lambda v: v.to_bytes(8, "little")
+    check(u64(index + 1) + s[8:], zgo.V_UNMATCHED_AMT_INDEX, a=index + 1, b=index)
+    if index < 3 * R - 1:
+        nxt = slices[index + 1]
+        check(s[:8] + nxt[8:lay["merkle"]] + s[lay["merkle"]:], zgo.V_UNMATCHED_AMT_INDEX, a=index, b=index + 1)
+        check(s[:lay["merkle"]] + nxt[lay["merkle"]:], zgo.V_UNMATCHED_MERKLE_INDEX, a=index, b=index + 1)
+    # AMT: WrongRow
+    row0 = (int.from_bytes(s[96:128], "little") + 1) % R_MOD
+    check(s[:96] + row0.to_bytes(32, "little") + s[128:], zgo.V_AMT_INCORRECT_PROOF, sub=zgo.P_INCONSISTENT,
+          a=coset, b=local)
+    # AMT: WrongIndex (row.index += 1)
+    check(s[:80] + u64(local + 1) + s[88:], zgo.V_AMT_UNMATCHED_COSET_INDEX, a=coset, b=local, c=local + 1)
+    # AMT: WrongCommitment (commitment + G1)
+    bad_com = mg.ser_g1(mg.g1_add(parse_g1(s[16:80]), mg.G1))
+    check(s[:16] + bad_com + s[80:], zgo.V_AMT_INCORRECT_COMMITMENT)
+    # AMT: IncorrectHighCommitment (high + G1)
+    h = lay["high"]
+    bad_high = mg.ser_g1(mg.g1_add(parse_g1(s[h:h + 64]), mg.G1))
+    check(s[:h] + bad_high + s[h + 64:], zgo.V_AMT_INCORRECT_PROOF, sub=zgo.P_LDT, a=coset, b=local)
+    # Merkle: WrongIndex (leaf_index += 1)
+    li = lay["leaf_index"]
+    check(s[:li] + u64(index + 1) + s[li + 8:], zgo.V_UNMATCHED_MERKLE_INDEX, a=index, b=index + 1)
+    # Merkle: WrongLocalRoot
+    lf = lay["leaf"]
+    check(s[:lf] + bump(s[lf:lf + 32]), zgo.V_MERKLE_INCORRECT_LOCAL_ROOT, a=index)
+    # Merkle: WrongProof (proof[0])
+    mp = lay["mproof"]
+    check(s[:mp] + bump(s[mp:mp + 32]) + s[mp + 32:], zgo.V_MERKLE_INCORRECT_PROOF, a=index)
+    # Merkle: WrongRoot (every root)
+    m = lay["merkle"]
+    roots = b"".join(bump(s[m + 32 * k:m + 32 * k + 32]) for k in range(3))
+    check(s[:m] + roots + s[m + 96:], zgo.V_MERKLE_INCORRECT_ROOT)
+
+
+def test_too_large_blob(oracle):
+    op = oracle.params(3, 5, 1)
+    max_raw = 31 * 256 - 4
+    oracle.encode(op, bytes(max_raw))
+    with pytest.raises(zgo.TooLargeBlob):
+        oracle.encode(op, bytes(max_raw + 1))
+
+
+def test_zero_payload_is_infinity(oracle):
+    op = oracle.params(3, 5, 1)
+    ob = oracle.encode(op, b"")
+    assert ob.commitment() == bytes(64)
+    assert ob.slice(0)[16:80] == bytes(63) + b"\x40"
+    rc, det = oracle.verify(op, ob.slice(5), ob.commitment(), ob.file_root())
+    assert rc == zgo.V_OK
+
+
+# ---- recovery (crates/recovery/src/data_poly.rs:164-256) -----------------------
+@pytest.fixture(scope="module")
+def recovery_blob(oracle):
+    lr, lc = 4, 5
+    op = oracle.params(lr, lc, 3)
+    payload = bytes(random.Random(9).randrange(256) for _ in range(31 * (1 << (lr + lc)) - 4))
+    data = oracle.encode(op, payload).data()
+    C = 1 << lc
+    rows = {i: data[i * C * 32:(i + 1) * C * 32] for i in range(3 << lr)}
+    return lr, lc, payload, rows
+
+
+def test_recovery_patterns(oracle, recovery_blob):
+    lr, lc, payload, rows = recovery_blob
+    R = 1 << lr
+    pats = [
+        range(1, 3 * R),
+        list(range(0, R)) + list(range(R + 1, 3 * R)),
+        range(R + 1, 3 * R),
+        range(3 * R - R, 3 * R),
+        range(0, R),
+        range(1, 3 * R, 2),
+    ]
+    rng = random.Random(4)
+    for k in (R, R + 1, 2 * R, 3 * R - 1, 3 * R):
+        pats.append(rng.sample(range(3 * R), k))
+    for p in pats:
+        rc, out = oracle.recover(lr, lc, {i: rows[i] for i in p})
+        assert rc == 0, (list(p)[:5], out)
+        assert out == payload
+
+
+def test_recovery_errors(oracle, recovery_blob):
+    lr, lc, payload, rows = recovery_blob
+    R = 1 << lr
+    few = {i: rows[i] for i in range(2 * R + 2, 3 * R)}               # R - 2 rows
+    assert oracle.recover(lr, lc, few) == (1, "Not enough valid lines")
+    over = {i: rows[i] for i in range(2 * R + 1, 3 * R)}
+    over[3 * R] = rows[0]                                                # row id >= BLOB_ROW_ENCODED
+    assert oracle.recover(lr, lc, over) == (2, "Cannot recover data: RowIdOverflow")
+    short = {i: rows[i] for i in range(R)}
+    short[R] = rows[R][:-1]                                              # malformed rows are dropped
+    rc, out = oracle.recover(lr, lc, short)
+    assert rc == 0 and out == payload
