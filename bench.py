@@ -106,7 +106,7 @@ def measured_peaks():
 
 def profile_traffic():
     """dram bytes per MSM launch from the committed ncu summary, if present."""
-    path = os.path.join(ROOT, "profiles", "msm_chunks_traffic.txt")
+    path = os.path.join(ROOT, "profiles", "msm_fb_accum_traffic.txt")
     try:
         with open(path) as f:
             for line in f:
@@ -325,7 +325,7 @@ def main():
     t_msm = phases["msm"] / 1000.0
     achieved = MSM_IMAD / t_msm / 1e9
     roofline = {
-        "kernel": "k_msm_chunks", "bound": "imad", "achieved": achieved, "peak": imad, "unit": "G IMAD/s",
+        "kernel": "k_fb_accum", "bound": "imad", "achieved": achieved, "peak": imad, "unit": "G IMAD/s",
         "frac": achieved / imad, "traffic": profile_traffic(),
         "note": "work = 1509949440 mixed adds/blob x 10 Fq mul x 264 IMAD (reference decomposition); "
                 "peak = live mad.lo.u32 probe on this GPU (of measured); traffic = dram bytes per launch "
