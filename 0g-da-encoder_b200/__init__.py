@@ -28,7 +28,8 @@ from . import build as _build
 
 __all__ = [
     "Dims", "RawData", "EncoderError", "TooLargeBlob", "ZgEncoderParams", "EncodedBlob",
-    "EncodeBlobReply", "EncoderService", "lib", "LIB_PATH", "C_ABI_FUNCTIONS",
+    "EncodeBlobReply", "EncoderService", "lib", "LIB_PATH", "C_ABI_FUNCTIONS", "recover_from_da_slice",
+    "RecoveryError",
 ]
 
 LIB_PATH = _build.LIB
@@ -36,6 +37,7 @@ _lib = None
 
 ZG_OK = 0
 ZG_ERR_TOO_LARGE_BLOB = 1
+ZG_ERR_RECOVERY = 2
 
 
 class _Config(ctypes.Structure):
@@ -81,6 +83,8 @@ _SIGS = {
     "zg_ctx_phase_times": (ctypes.c_int, [_P, ctypes.POINTER(ctypes.c_float), ctypes.c_int]),
     "zg_ctx_launches": (ctypes.c_uint64, [_P]),
     "zg_probe_imad": (ctypes.c_int, [ctypes.c_int, ctypes.POINTER(ctypes.c_double)]),
+    "zg_recover": (ctypes.c_int, [_P, ctypes.POINTER(ctypes.c_uint64), ctypes.POINTER(ctypes.c_char_p),
+                                  ctypes.POINTER(_SZ), _SZ, ctypes.c_char_p, _SZ, ctypes.POINTER(_SZ)]),
     "zg_msm_chunks": (ctypes.c_int, [_P, _P, ctypes.c_uint32, ctypes.c_uint32, ctypes.c_uint32, _P, _P]),
     "zg_msm_chunks_noalloc": (ctypes.c_int, [_P, _P, ctypes.c_uint32, ctypes.c_uint32, ctypes.c_uint32, _P, _P]),
     "zg_ntt": (ctypes.c_int, [_P, ctypes.c_uint32, ctypes.c_uint32, ctypes.c_int, ctypes.c_uint32, _P]),
@@ -349,6 +353,28 @@ class EncodedBlob:
 
     def get_data(self) -> bytes:
         return self._data
+
+
+class RecoveryError(Exception):
+    """recover_from_da_slice's Err(String); the message is the reference's text."""
+
+
+def recover_from_da_slice(params: ZgEncoderParams, slices: dict) -> bytes:
+    """crates/recovery/src/lib.rs:15-43: {row index: 32-byte-element row bytes}
+    -> original payload (raises RecoveryError)."""
+    L = lib()
+    ids = sorted(slices)
+    n = len(ids)
+    arr = (ctypes.c_uint64 * n)(*ids)
+    bufs = (ctypes.c_char_p * n)(*[slices[i] for i in ids])
+    lens = (ctypes.c_size_t * n)(*[len(slices[i]) for i in ids])
+    out = ctypes.create_string_buffer(params.dims.max_raw_data_size)
+    out_len = ctypes.c_size_t()
+    rc = L.zg_recover(params.handle, arr, bufs, lens, n, out, len(out), ctypes.byref(out_len))
+    if rc == ZG_ERR_RECOVERY:
+        raise RecoveryError(L.zg_last_error().decode())
+    _check(rc)
+    return out.raw[:out_len.value]
 
 
 class EncoderService:

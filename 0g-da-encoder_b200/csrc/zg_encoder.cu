@@ -17,6 +17,7 @@
 
 #include "../../include/zg_encoder.h"
 #include "zg_kernels.cuh"
+#include "zg_recover.cuh"
 
 using namespace zg;
 
@@ -230,6 +231,17 @@ struct zg_ctx {
   size_t slice_size = 0;
   uint8_t* file_root = nullptr;
   uint8_t* h_in = nullptr;  // pinned staging for payloads
+  // recovery buffers and tables, allocated on the first zg_recover call
+  bool rec_ready = false;
+  Fr *rec_ginv = nullptr, *rec_kpow = nullptr, *rec_kinv = nullptr, *rec_wpow = nullptr, *rec_zinv = nullptr,
+     *rec_zw = nullptr;
+  Fr *rec_V = nullptr, *rec_W = nullptr;
+  uint8_t* rec_rows = nullptr;   // device copy of the received rows
+  uint8_t* rec_raw = nullptr;    // device RawData
+  uint32_t* rec_ids = nullptr;
+  uint16_t* rec_erased = nullptr;
+  uint32_t* rec_err = nullptr;
+  uint8_t* h_rec = nullptr;      // pinned staging (rows in, RawData out)
   // measurement: optional per-phase events and a count of kernel launches
   bool profiling = false;
   cudaEvent_t ev[6] = {nullptr, nullptr, nullptr, nullptr, nullptr, nullptr};
@@ -606,6 +618,47 @@ __global__ void k_imad_probe(uint32_t* sink, uint32_t iters, uint32_t seed) {
   if (x == 0x12345678u) sink[0] = x;
 }
 
+// Recovery set-up: tables for the factored decode (see zg_recover.cuh) and
+// buffers sized for 3R received rows.
+int rec_setup(zg_ctx* c) {
+  if (c->rec_ready) return 0;
+  const int lr = c->lr, lc = c->lc, lm = c->lr + 2;
+  const size_t R = c->R, C = c->C, M = size_t(1) << lm;
+  if (lr > 10) return fail(ZG_ERR_INVALID_ARG, "recovery supports log_row <= 10");
+  std::vector<Fr> ginv;
+  Fr cinv = host_fr_from_u32((uint32_t)C).inverse();
+  for (int cs = 0; cs < 3; ++cs) {
+    Fr g = cs ? coset_factor(lr + lc, cs).inverse() : Fr::one();
+    std::vector<Fr> t = pow_table(g, C);
+    for (auto& x : t) x = x * cinv;
+    ginv.insert(ginv.end(), t.begin(), t.end());
+  }
+  Fr k = host_fr_from_u32(5);  // generator of Fr*: never a root of unity of the domain
+  Fr minv = host_fr_from_u32((uint32_t)M).inverse();
+  std::vector<Fr> kp = pow_table(k, M), ki = pow_table(k.inverse(), M);
+  for (auto& x : kp) x = x * minv;
+  for (auto& x : ki) x = x * minv;
+  int rc = 0;
+  if ((rc = upload(&c->rec_ginv, ginv)) || (rc = upload(&c->rec_kpow, kp)) || (rc = upload(&c->rec_kinv, ki)) ||
+      (rc = upload(&c->rec_wpow, pow_table(fr_root(lm), M))))
+    return rc;
+  ZG_CK(cudaMalloc(&c->rec_zinv, M * sizeof(Fr)));
+  ZG_CK(cudaMalloc(&c->rec_zw, M * sizeof(Fr)));
+  ZG_CK(cudaMalloc(&c->rec_V, M * C * sizeof(Fr)));
+  ZG_CK(cudaMalloc(&c->rec_W, R * C * sizeof(Fr)));
+  ZG_CK(cudaMalloc(&c->rec_rows, 3 * R * C * 32));
+  ZG_CK(cudaMalloc(&c->rec_raw, c->max_blob + 16));
+  ZG_CK(cudaMalloc(&c->rec_ids, 3 * R * sizeof(uint32_t)));
+  ZG_CK(cudaMalloc(&c->rec_erased, M * sizeof(uint16_t)));
+  ZG_CK(cudaMalloc(&c->rec_err, sizeof(uint32_t)));
+  ZG_CK(cudaMallocHost(&c->h_rec, std::max(3 * R * C * 32, c->max_blob + 16)));
+  ZG_CK(cudaFuncSetAttribute(k_rec_rows, cudaFuncAttributeMaxDynamicSharedMemorySize, 227 * 1024));
+  ZG_CK(cudaFuncSetAttribute(k_rec_cols, cudaFuncAttributeMaxDynamicSharedMemorySize, 227 * 1024));
+  ZG_CK(cudaFuncSetAttribute(k_rec_out, cudaFuncAttributeMaxDynamicSharedMemorySize, 227 * 1024));
+  c->rec_ready = true;
+  return 0;
+}
+
 }  // namespace
 
 extern "C" {
@@ -676,6 +729,10 @@ void zg_ctx_destroy(zg_ctx* c) {
   if (c->done) cudaEventSynchronize(c->done);  // work queued on caller streams
   if (c->stream) cudaStreamSynchronize(c->stream);
   free_twiddles(&c->tw);
+  void* rp[] = {c->rec_zw, c->rec_ginv, c->rec_kpow, c->rec_kinv, c->rec_wpow, c->rec_zinv, c->rec_V, c->rec_W,
+                c->rec_rows, c->rec_raw, c->rec_ids, c->rec_erased, c->rec_err};
+  for (void* p : rp) if (p) cudaFree(p);
+  if (c->h_rec) cudaFreeHost(c->h_rec);
   void* ps[] = {c->tab, c->raw, c->enc, c->T1, c->Bc, c->win, c->part, c->nodes, c->amt,
                 c->tree, c->tree_off_d, c->slices, c->file_root, c->fb_offs, c->fb_ents, c->fb_T, c->fb_S, c->fb_gbuf};
   for (void* p : ps) if (p) cudaFree(p);
@@ -931,6 +988,93 @@ int zg_msm_chunks_noalloc(const void* d_bases, const void* d_scalars, uint32_t l
   k_msm_combine<<<nblk(count, 64), 64, 0, s>>>(win, part, (uint32_t)count);
   k_serialize_nodes<<<nblk(count, 128), 128, 0, s>>>(part, (uint8_t*)d_out, (uint32_t)count);
   return check_launch();
+}
+
+int zg_recover(zg_ctx* c, const uint64_t* row_ids, const uint8_t* const* rows, const size_t* row_lens, size_t n,
+               uint8_t* out, size_t out_cap, size_t* out_len) {
+  if (!c || (n && (!row_ids || !rows || !row_lens)) || !out_len) return fail(ZG_ERR_INVALID_ARG, "null argument");
+  const size_t R = c->R, C = c->C, M = 4 * R;
+  const int lr = c->lr, lc = c->lc, lm = lr + 2;
+  // raw_slice_to_line drops rows of the wrong length; a map keeps one row per id
+  std::map<uint64_t, const uint8_t*> valid;
+  for (size_t i = 0; i < n; ++i)
+    if (row_lens[i] == 32 * C) valid[row_ids[i]] = rows[i];
+  // The reference converts every row (and panics on a value >= r) before it
+  // counts them, so a non-canonical row outranks the two input errors. On the
+  // good path the rows are checked on the device.
+  auto any_noncanonical = [&]() {
+    for (auto& kv : valid)
+      for (size_t j = 0; j < C; ++j) {
+        Fr x, d;
+        memcpy(x.v, kv.second + 32 * j, 32);
+        if (!Fr::sub_raw(d, x, Fr::modulus())) return true;
+      }
+    return false;
+  };
+  const char* input_err = nullptr;
+  if (valid.size() < R)
+    input_err = "Not enough valid lines";
+  else if (valid.rbegin()->first >= 3 * R)
+    input_err = "Cannot recover data: RowIdOverflow";
+  if (input_err) {
+    if (any_noncanonical()) return fail(ZG_ERR_RECOVERY, "Non-canonical field element in slice");
+    return fail(ZG_ERR_RECOVERY, input_err);
+  }
+  std::lock_guard<std::mutex> g(c->mu);
+  ZG_CK(cudaSetDevice(c->device));
+  int rc = rec_setup(c);
+  if (rc) return rc;
+  cudaStream_t s = c->stream;
+  ZG_CK(cudaStreamWaitEvent(s, c->done, 0));
+  // received rows -> pinned staging -> device; erased domain points (incl. the virtual coset)
+  std::vector<uint32_t> ids;
+  std::vector<uint8_t> known(M, 0);
+  size_t k = 0;
+  for (auto& kv : valid) {
+    memcpy(c->h_rec + k * 32 * C, kv.second, 32 * C);
+    ids.push_back((uint32_t)kv.first);
+    const uint32_t cs = (uint32_t)(kv.first >> lr), r = (uint32_t)(kv.first & (R - 1));
+    known[4 * r + (cs == 1 ? 2 : (cs == 2 ? 1 : cs))] = 1;
+    ++k;
+  }
+  std::vector<uint16_t> erased;
+  for (size_t i = 0; i < M; ++i)
+    if (!known[i]) erased.push_back((uint16_t)i);
+  ZG_CK(cudaMemcpyAsync(c->rec_rows, c->h_rec, k * 32 * C, cudaMemcpyHostToDevice, s));
+  ZG_CK(cudaMemcpyAsync(c->rec_ids, ids.data(), k * sizeof(uint32_t), cudaMemcpyHostToDevice, s));
+  ZG_CK(cudaMemcpyAsync(c->rec_erased, erased.data(), erased.size() * sizeof(uint16_t), cudaMemcpyHostToDevice, s));
+  ZG_CK(cudaMemsetAsync(c->rec_V, 0, M * C * sizeof(Fr), s));
+  ZG_CK(cudaMemsetAsync(c->rec_err, 0, sizeof(uint32_t), s));
+  const Twiddles* tm = cached_twiddles(0, lm);
+  if (!tm) return ZG_ERR_CUDA;
+  k_rec_rows<<<(unsigned)k, 256, C * sizeof(Fr), s>>>(c->rec_rows, c->rec_ids, c->rec_V, lr, lc, c->tw.twi_c,
+                                                       c->rec_ginv, c->tw.wni_lo, c->tw.wni_hi, c->rec_err);
+  k_rec_zinv<<<nblk(M, 128), 128, 0, s>>>(c->rec_erased, (uint32_t)erased.size(), c->rec_wpow, host_fr_from_u32(5),
+                                          c->rec_zw, c->rec_zinv, (uint32_t)M);
+  k_rec_cols<<<(unsigned)C, 256, (M + R) * sizeof(Fr), s>>>(c->rec_V, c->rec_W, lr, lc, tm->twf_c, tm->twi_c,
+                                                             c->rec_kpow, c->rec_kinv, c->rec_zw, c->rec_zinv, c->tw.twf_r,
+                                                             c->tw.wn_lo, c->tw.wn_hi, c->rec_err);
+  k_rec_out<<<(unsigned)R, 256, C * sizeof(Fr), s>>>(c->rec_W, c->rec_raw, lc, c->tw.twf_c, c->rec_err);
+  if ((rc = check_launch())) return rc;
+  uint32_t err = 0;
+  ZG_CK(cudaMemcpyAsync(&err, c->rec_err, sizeof(uint32_t), cudaMemcpyDeviceToHost, s));
+  ZG_CK(cudaMemcpyAsync(c->h_rec, c->rec_raw, c->max_blob, cudaMemcpyDeviceToHost, s));
+  ZG_CK(cudaEventRecord(c->done, s));
+  ZG_CK(cudaStreamSynchronize(s));
+  // the reference panics on these two (from_bigint(...).unwrap(), the degree assert)
+  if (err & 1) return fail(ZG_ERR_RECOVERY, "Non-canonical field element in slice");
+  if (err & 2) return fail(ZG_ERR_RECOVERY, "Inconsistent rows (degree check)");
+  // RawBlob -> RawData (crates/encoder/src/raw_blob.rs:42-58, raw_data.rs:25-38)
+  if (err & 4) return fail(ZG_ERR_RECOVERY, "Incorrect scalar");
+  uint32_t l32;
+  memcpy(&l32, c->h_rec + c->max_raw, 4);
+  if (l32 > c->max_raw) return fail(ZG_ERR_RECOVERY, "Incorrect length field");
+  for (size_t i = l32; i < c->max_raw; ++i)
+    if (c->h_rec[i]) return fail(ZG_ERR_RECOVERY, "Non zero in padding range");
+  if (out_cap < l32) return fail(ZG_ERR_INVALID_ARG, "output buffer too small");
+  memcpy(out, c->h_rec, l32);
+  *out_len = l32;
+  return ZG_OK;
 }
 
 int zg_ntt(void* d_data, uint32_t log_n, uint32_t batch, int inverse, uint32_t coset_idx, void* stream) {

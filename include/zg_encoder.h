@@ -31,6 +31,7 @@ extern "C" {
 
 #define ZG_OK 0
 #define ZG_ERR_TOO_LARGE_BLOB 1
+#define ZG_ERR_RECOVERY 2
 #define ZG_ERR_INVALID_ARG (-1)
 #define ZG_ERR_CUDA (-2)
 #define ZG_ERR_PARAMS (-3)
@@ -103,6 +104,19 @@ uint64_t zg_ctx_launches(const zg_ctx* ctx);
 /* Integer multiply-add rate of the device (independent mad.lo.u32 chains),
  * in 1e9 per second: the denominator of the MSM roofline. */
 int zg_probe_imad(int device, double* gimad_per_s);
+
+/* recover_from_da_slice (crates/recovery/src/lib.rs:15-43): original payload
+ * bytes from any >= R encoded rows. rows[i] (host memory, row_lens[i] bytes)
+ * is encoded row row_ids[i] (0 <= id < 3R) as 32-byte canonical elements, the
+ * EncodedSlice::merkle_row() bytes. Rows of the wrong length are dropped and
+ * one row is kept per id, as the reference's BTreeMap input does. Returns
+ * ZG_OK with the payload in out[0..*out_len), or ZG_ERR_RECOVERY with the
+ * reference's error text in zg_last_error(): "Not enough valid lines",
+ * "Cannot recover data: RowIdOverflow", "Incorrect scalar", "Incorrect length
+ * field", "Non zero in padding range"; rows that are not one codeword or hold
+ * a value >= r (the reference panics) give their own messages. */
+int zg_recover(zg_ctx* ctx, const uint64_t* row_ids, const uint8_t* const* rows, const size_t* row_lens, size_t n,
+               uint8_t* out, size_t out_cap, size_t* out_len);
 
 /* Kernel-level entry points (device pointers, stream-ordered on `stream`).
  * zg_msm_chunks: the AMT plugin's MSM decomposition (prove_gpu.rs:55-87):

@@ -345,6 +345,21 @@ def test_production_slices_verify(prod, oracle):
         assert rc == zgo.V_OK, (i, rc, det)
 
 
+def test_production_recovery_round_trip(prod, gpu_pkg):
+    """1024 x 1024 blob: the payload back from a seeded random half of the
+    3072 rows, from the two parity cosets alone and from exactly R rows."""
+    params, _, payload, reply = prod
+    R, C = 1024, 1024
+    data = reply.encoded_data
+    rows = {i: data[i * C * 32:(i + 1) * C * 32] for i in range(3 * R)}
+    rnd = random.Random(21)
+    for ids in (rnd.sample(range(3 * R), 3 * R // 2), range(R, 3 * R), rnd.sample(range(3 * R), R)):
+        assert gpu_pkg.recover_from_da_slice(params, {i: rows[i] for i in ids}) == payload
+    bad = {i: rows[i] for i in rnd.sample(range(3 * R), R - 1)}
+    with pytest.raises(gpu_pkg.RecoveryError, match="Not enough valid lines"):
+        gpu_pkg.recover_from_da_slice(params, bad)
+
+
 def test_encode_matches_golden_fixture(gpu_pkg):
     """The CUDA path against the independent pure-Python restatement's bytes
     (tests/golden/make_golden.py, 8 x 32 blob)."""

@@ -280,3 +280,17 @@ def test_recovery_errors(oracle, recovery_blob):
     short[R] = rows[R][:-1]                                              # malformed rows are dropped
     rc, out = oracle.recover(lr, lc, short)
     assert rc == 0 and out == payload
+
+
+def test_recovery_error_branches(oracle):
+    """Codewords of invalid RawData and invalid inputs (tests/recovery_cases.py)."""
+    from recovery_cases import bad_codewords
+    lr, lc = 4, 5
+    op = oracle.params(lr, lc, 3)
+    cases = bad_codewords(lambda p: oracle.encode(op, p).data(), lr, lc)
+    for name, rows, expected in cases:
+        rc, out = oracle.recover(lr, lc, rows)
+        if isinstance(expected, bytes):
+            assert (rc, out) == (0, expected), name
+        else:
+            assert rc and out == expected, (name, rc, out)
