@@ -29,7 +29,7 @@ from . import build as _build
 __all__ = [
     "Dims", "RawData", "EncoderError", "TooLargeBlob", "ZgEncoderParams", "EncodedBlob",
     "EncodeBlobReply", "EncoderService", "lib", "LIB_PATH", "C_ABI_FUNCTIONS", "recover_from_da_slice",
-    "RecoveryError",
+    "RecoveryError", "Ticket",
 ]
 
 LIB_PATH = _build.LIB
@@ -38,6 +38,9 @@ _lib = None
 ZG_OK = 0
 ZG_ERR_TOO_LARGE_BLOB = 1
 ZG_ERR_RECOVERY = 2
+ZG_ERR_TIMEOUT = 3
+ZG_REQ_ENCODE = 0
+ZG_REQ_RECOVER = 1
 
 
 class _Config(ctypes.Structure):
@@ -64,7 +67,20 @@ class _DeviceBlob(ctypes.Structure):
 
 _P = ctypes.c_void_p
 _SZ = ctypes.c_size_t
+class _Request(ctypes.Structure):
+    """zg_request (include/zg_encoder.h)."""
+    _fields_ = [("kind", ctypes.c_int), ("data", ctypes.c_void_p), ("len", ctypes.c_size_t),
+                ("require_data", ctypes.c_int), ("row_ids", ctypes.POINTER(ctypes.c_uint64)),
+                ("rows", ctypes.POINTER(ctypes.c_char_p)), ("row_lens", ctypes.POINTER(ctypes.c_size_t)),
+                ("n_rows", ctypes.c_size_t)]
+
+
 _SIGS = {
+    "zg_submit": (ctypes.c_int, [_P, ctypes.POINTER(_Request), ctypes.POINTER(ctypes.c_uint64)]),
+    "zg_wait": (ctypes.c_int, [_P, ctypes.c_uint64, ctypes.c_int64, ctypes.POINTER(_P)]),
+    "zg_reply_payload": (_P, [_P, ctypes.POINTER(_SZ)]),
+    "zg_encode_batch": (ctypes.c_int, [_P, _SZ, ctypes.POINTER(ctypes.c_void_p), ctypes.POINTER(_SZ), ctypes.c_int,
+                                       ctypes.POINTER(_P)]),
     "zg_ctx_create": (ctypes.c_int, [ctypes.POINTER(_Config), ctypes.POINTER(_P)]),
     "zg_ctx_destroy": (None, [_P]),
     "zg_ctx_warmup": (ctypes.c_int, [_P]),
@@ -118,6 +134,10 @@ def _check(rc):
     msg = lib().zg_last_error().decode(errors="replace")
     if rc == ZG_ERR_TOO_LARGE_BLOB:
         raise TooLargeBlob.from_message(msg)
+    if rc == ZG_ERR_RECOVERY:
+        raise RecoveryError(msg)
+    if rc == ZG_ERR_TIMEOUT:
+        raise TimeoutError(msg)
     raise RuntimeError(f"zg_encoder error {rc}: {msg}")
 
 
@@ -295,10 +315,10 @@ class EncodeBlobReply:
     encoded_slice: List[bytes] = field(default_factory=list)
 
 
-def _encode_raw(params: ZgEncoderParams, data: bytes, require_data: bool):
+def _read_reply(r):
+    """(version, commitment, storage root, encoded data, coset roots, slices)
+    copied out of a zg_reply, which is then freed."""
     L = lib()
-    r = ctypes.c_void_p()
-    _check(L.zg_encode(params.handle, data, len(data), 1 if require_data else 0, ctypes.byref(r)))
     try:
         n = ctypes.c_size_t()
 
@@ -317,6 +337,12 @@ def _encode_raw(params: ZgEncoderParams, data: bytes, require_data: bool):
         return L.zg_reply_version(r), com, root, edata, roots, slices
     finally:
         L.zg_reply_free(r)
+
+
+def _encode_raw(params: ZgEncoderParams, data: bytes, require_data: bool):
+    r = ctypes.c_void_p()
+    _check(lib().zg_encode(params.handle, data, len(data), 1 if require_data else 0, ctypes.byref(r)))
+    return _read_reply(r)
 
 
 class EncodedBlob:
@@ -386,3 +412,80 @@ class EncoderService:
     def process_data(self, data: bytes, require_data: bool) -> EncodeBlobReply:
         version, com, root, edata, _, slices = _encode_raw(self.params, data, require_data)
         return EncodeBlobReply(version, com, root, edata, slices)
+
+    def process_batch(self, payloads, require_data: bool) -> List[EncodeBlobReply]:
+        """Many process_data calls through the pipelined path (zg_encode_batch);
+        replies are bit-identical to process_data's."""
+        n = len(payloads)
+        ptrs = (ctypes.c_void_p * n)(*[_addr(p) for p in payloads])
+        lens = (ctypes.c_size_t * n)(*[_nbytes(p) for p in payloads])
+        outs = (ctypes.c_void_p * n)()
+        _check(lib().zg_encode_batch(self.params.handle, n, ptrs, lens, 1 if require_data else 0, outs))
+        replies = []
+        for i in range(n):
+            version, com, root, edata, _, slices = _read_reply(ctypes.c_void_p(outs[i]))
+            replies.append(EncodeBlobReply(version, com, root, edata, slices))
+        return replies
+
+    def submit(self, data, require_data: bool) -> "Ticket":
+        """Queue one encode (zg_submit); `data` is bytes or (pointer, length)."""
+        q = _Request()
+        q.kind = ZG_REQ_ENCODE
+        q.data = _addr(data)
+        q.len = _nbytes(data)
+        q.require_data = 1 if require_data else 0
+        return self._submit(q, (data,))
+
+    def submit_recover(self, slices: dict) -> "Ticket":
+        """Queue one recover_from_da_slice (crates/recovery/src/lib.rs:15-43)."""
+        ids = sorted(slices)
+        n = len(ids)
+        arr = (ctypes.c_uint64 * n)(*ids)
+        bufs = (ctypes.c_char_p * n)(*[slices[i] for i in ids])
+        lens = (ctypes.c_size_t * n)(*[len(slices[i]) for i in ids])
+        q = _Request()
+        q.kind = ZG_REQ_RECOVER
+        q.row_ids = arr
+        q.rows = bufs
+        q.row_lens = lens
+        q.n_rows = n
+        return self._submit(q, (slices, arr, bufs, lens))
+
+    def _submit(self, q, keep):
+        t = ctypes.c_uint64()
+        _check(lib().zg_submit(self.params.handle, ctypes.byref(q), ctypes.byref(t)))
+        return Ticket(t.value, q.kind, (q,) + keep)
+
+    def wait(self, ticket: "Ticket", timeout_ms: int = -1):
+        """The result of a submitted request: an EncodeBlobReply, or the
+        recovered payload bytes; raises the request's error."""
+        r = ctypes.c_void_p()
+        _check(lib().zg_wait(self.params.handle, ticket.id, timeout_ms, ctypes.byref(r)))
+        ticket.refs = None
+        if ticket.kind == ZG_REQ_RECOVER:
+            n = ctypes.c_size_t()
+            try:
+                p = lib().zg_reply_payload(r, ctypes.byref(n))
+                return ctypes.string_at(p, n.value) if n.value else b""
+            finally:
+                lib().zg_reply_free(r)
+        version, com, root, edata, _, slices = _read_reply(r)
+        return EncodeBlobReply(version, com, root, edata, slices)
+
+
+@dataclass
+class Ticket:
+    """A submitted request; its input buffers stay referenced until wait()."""
+    id: int
+    kind: int
+    refs: tuple = ()
+
+
+def _addr(data):
+    if isinstance(data, tuple):
+        return data[0]
+    return ctypes.cast(ctypes.c_char_p(data), ctypes.c_void_p).value if len(data) else None
+
+
+def _nbytes(data):
+    return data[1] if isinstance(data, tuple) else len(data)

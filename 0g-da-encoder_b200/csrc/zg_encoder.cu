@@ -8,10 +8,13 @@
 #include <cuda_runtime.h>
 #include <dirent.h>
 
+#include <condition_variable>
 #include <cstdio>
 #include <cstring>
 #include <map>
 #include <mutex>
+#include <thread>
+#include <deque>
 #include <string>
 #include <vector>
 
@@ -195,6 +198,11 @@ constexpr uint32_t ZG_NOALLOC_MAX_MSMS = 1024;
 static __device__ __align__(256) uint8_t g_noalloc_scratch[(size_t)ZG_NOALLOC_MAX_MSMS * (MSM_WINDOWS + 1) *
                                                            sizeof(XYZZ)];
 
+namespace {
+struct Engine;
+void engine_shutdown(Engine* e);
+}  // namespace
+
 struct zg_ctx {
   int device = 0;
   int lr = 0, lc = 0, L = 0;
@@ -250,6 +258,9 @@ struct zg_ctx {
   cudaEvent_t done = nullptr;
   uint64_t launches = 0;
   std::mutex mu;
+  // request pipeline (zg_submit / zg_wait / zg_encode_batch), started on first use
+  Engine* eng = nullptr;
+  std::mutex eng_mu;
 };
 
 // Process-wide pool of page-locked reply buffers: pinning ~200 MB per reply
@@ -289,6 +300,7 @@ struct zg_reply {
   size_t data_len = 0;
   uint8_t* slices = nullptr;  // pinned
   size_t slice_size = 0, nslices = 0;
+  std::vector<uint8_t> payload;  // recovered bytes (recovery requests)
 };
 
 namespace {
@@ -448,32 +460,63 @@ int merkle_levels(const uint8_t* items, size_t n_items, uint8_t* tree, const std
   return check_launch();
 }
 
-// the full per-blob pipeline on device; d_data holds `len` payload bytes
-int encode_device_locked(zg_ctx* c, const uint8_t* d_data, size_t len, cudaStream_t s) {
+// Per-blob inputs and outputs: the payload, the encoded data, the Merkle
+// tree, the serialized AMT nodes, the slices and the file root. The context
+// owns one set (the plain path); the request pipeline owns two more, so one
+// blob's copies overlap the other's compute.
+struct BlobBufs {
+  uint8_t* raw = nullptr;
+  uint64_t* d_len = nullptr;  // payload length, for graph launches
+  uint8_t* enc = nullptr;
+  uint8_t* tree = nullptr;
+  uint8_t* amt = nullptr;
+  uint8_t* slices = nullptr;
+  uint8_t* file_root = nullptr;
+};
+
+BlobBufs ctx_bufs(zg_ctx* c) {
+  BlobBufs b;
+  b.raw = c->raw;
+  b.enc = c->enc;
+  b.tree = c->tree;
+  b.amt = c->amt;
+  b.slices = c->slices;
+  b.file_root = c->file_root;
+  return b;
+}
+
+// Kernel launches of one encode: 3 RS passes, leaves + tree_depth parent
+// levels, file root, MSM (sort, accumulate, combine or chunks, combine),
+// trees, serialisation, slices.
+uint64_t launches_per_encode(const zg_ctx* c) { return 3 + (uint64_t)c->tree_depth + 1 + 1 + (c->fb ? 3 : 2) + 1 + 1 + 1; }
+
+// The per-blob pipeline on the device, launches only. The payload is `len`
+// bytes at b.raw, or *b.d_len bytes when `by_device_len` (graph capture).
+int encode_launches(zg_ctx* c, const BlobBufs& b, size_t len, bool by_device_len, cudaStream_t s, bool marks) {
   const int lr = c->lr, lc = c->lc;
   const size_t R = c->R, C = c->C, N = c->N;
   auto mark = [&](int k) {
-    if (c->profiling) cudaEventRecord(c->ev[k], s);
+    if (marks && c->profiling) cudaEventRecord(c->ev[k], s);
   };
-  if (cudaStreamWaitEvent(s, c->done, 0) != cudaSuccess) return fail(ZG_ERR_CUDA, "stream wait failed");
   mark(0);
   // RS extension: rows iNTT, column passes, rows NTT
   k_rows_from_raw<<<(unsigned)R, 256, C * sizeof(Fr) + 31 * C, s>>>(
-      d_data, len, c->max_raw, lr, lc, c->enc, c->T1, c->tw.twi_c, c->tw.wni_lo, c->tw.wni_hi);
+      b.raw, len, by_device_len ? b.d_len : nullptr, c->max_raw, lr, lc, b.enc, c->T1, c->tw.twi_c, c->tw.wni_lo,
+      c->tw.wni_hi);
   k_cols<<<nblk(C, COLS_PER_BLOCK), 256, 2 * R * sizeof(Fr), s>>>(c->T1, c->Bc, lr, lc, c->tw.twi_r, c->tw.twf_r,
                                                                    c->tw.gs_lo, c->tw.gs_hi, c->tw.wn_lo,
                                                                    c->tw.wn_hi);
-  k_rows_ntt<<<dim3((unsigned)R, 2), 256, C * sizeof(Fr), s>>>(c->Bc, c->enc, lr, lc, c->tw.twf_c);
+  k_rows_ntt<<<dim3((unsigned)R, 2), 256, C * sizeof(Fr), s>>>(c->Bc, b.enc, lr, lc, c->tw.twf_c);
   int rc = check_launch();
   if (rc) return rc;
   mark(1);
   // Merkle tree over the encoded data and the file root
-  if ((rc = merkle_levels(c->enc, 3 * N, c->tree, c->tree_off, c->tree_depth, s))) return rc;
-  k_file_root<<<1, 32, 0, s>>>(c->tree + c->tree_off[0], c->file_root);
+  if ((rc = merkle_levels(b.enc, 3 * N, b.tree, c->tree_off, c->tree_depth, s))) return rc;
+  k_file_root<<<1, 32, 0, s>>>(b.tree + c->tree_off[0], b.file_root);
   mark(2);
   // AMT: per-chunk MSMs, trees, serialisation
   if (c->fb) {
-    k_fb_sort<<<dim3((unsigned)R, 3), 256, fb_sort_smem_bytes(lc), s>>>(c->enc, c->fb_offs, c->fb_ents, lr, lc, 1,
+    k_fb_sort<<<dim3((unsigned)R, 3), 256, fb_sort_smem_bytes(lc), s>>>(b.enc, c->fb_offs, c->fb_ents, lr, lc, 1,
                                                                          N);
     FbAccArgs fa;
     fa.tab = c->tab;
@@ -490,7 +533,7 @@ int encode_device_locked(zg_ctx* c, const uint8_t* d_data, size_t len, cudaStrea
     k_fb_combine<<<nblk(units, 64), 64, 0, s>>>(c->fb_T, c->fb_S, c->part, lr, c->L, units);
   } else {
     MsmChunkArgs a;
-    a.scalars = c->enc;
+    a.scalars = b.enc;
     a.bases = c->tab;
     a.win = c->win;
     a.lr = lr;
@@ -507,24 +550,33 @@ int encode_device_locked(zg_ctx* c, const uint8_t* d_data, size_t len, cudaStrea
   }
   k_amt_tree<<<dim3((unsigned)c->L, 3), 256, 0, s>>>(c->part, c->nodes, lr, c->L);
   const uint32_t nn = (uint32_t)(3 * (4 * R - 2));
-  k_serialize_nodes<<<nblk(nn, 128), 128, 0, s>>>(c->nodes, c->amt, nn);
+  k_serialize_nodes<<<nblk(nn, 128), 128, 0, s>>>(c->nodes, b.amt, nn);
   mark(4);
   SliceArgs sa;
-  sa.enc = c->enc;
-  sa.amt = c->amt;
-  sa.tree = c->tree;
+  sa.enc = b.enc;
+  sa.amt = b.amt;
+  sa.tree = b.tree;
   sa.tree_off = c->tree_off_d;
-  sa.out = c->slices;
+  sa.out = b.slices;
   sa.lr = lr;
   sa.lc = lc;
   sa.slice_size = c->slice_size;
   k_slices<<<(unsigned)(3 * R), 256, 0, s>>>(sa);
   mark(5);
-  // 3 RS passes, leaves + tree_depth parent levels, file root, MSM (sort,
-  // accumulate, combine or chunks, combine), trees, serialisation, slices
-  c->launches += 3 + (uint64_t)c->tree_depth + 1 + 1 + (c->fb ? 3 : 2) + 1 + 1 + 1;
-  if (cudaEventRecord(c->done, s) != cudaSuccess) return fail(ZG_ERR_CUDA, "event record failed");
   return check_launch();
+}
+
+// the full per-blob pipeline on the context's own buffers; d_data holds `len`
+// payload bytes
+int encode_device_locked(zg_ctx* c, const uint8_t* d_data, size_t len, cudaStream_t s) {
+  if (cudaStreamWaitEvent(s, c->done, 0) != cudaSuccess) return fail(ZG_ERR_CUDA, "stream wait failed");
+  BlobBufs b = ctx_bufs(c);
+  b.raw = const_cast<uint8_t*>(d_data);
+  int rc = encode_launches(c, b, len, false, s, true);
+  if (rc) return rc;
+  c->launches += launches_per_encode(c);
+  if (cudaEventRecord(c->done, s) != cudaSuccess) return fail(ZG_ERR_CUDA, "event record failed");
+  return 0;
 }
 
 std::mutex g_ntt_mu;
@@ -659,6 +711,292 @@ int rec_setup(zg_ctx* c) {
   return 0;
 }
 
+// ---------------------------------------------------------------------------
+// Request pipeline (zg_submit / zg_wait / zg_encode_batch). Two blob slots,
+// each with its own input and output buffers, alternate: the payload copy of
+// one blob (copy-in stream) and the reply copy of the other (copy-out stream)
+// overlap the compute of a third on the context's stream. Each slot's
+// compute sequence is captured once as a CUDA graph (the payload length is
+// read from device memory). One issuer thread launches requests in arrival
+// order; one completion thread waits for each slot's copy-out in the same
+// order and finishes its reply. Recovery requests run between encodes, after
+// the slots drain.
+struct Request {
+  zg_request req{};
+  zg_reply* reply = nullptr;
+  int status = 0;
+  std::string error;
+  bool done = false;
+};
+
+struct Slot {
+  BlobBufs b;
+  uint8_t* h_stage = nullptr;  // pinned payload staging for pageable callers
+  uint8_t* h_small = nullptr;  // pinned: [0,8) length, [8,200) coset commitments, [200,296) roots, [296,328) file root
+  cudaEvent_t ev_in = nullptr, ev_comp = nullptr, ev_out = nullptr;
+  cudaGraphExec_t graph = nullptr;
+  Request* req = nullptr;  // reserved for / in flight in this slot
+};
+
+struct Engine {
+  zg_ctx* c = nullptr;
+  Slot slot[2];
+  cudaStream_t h2d = nullptr, d2h = nullptr;
+  std::mutex mu;  // queue, slots, tickets
+  std::condition_variable cv;
+  std::deque<Request*> queue;
+  std::deque<int> inflight;  // slots in issue order
+  std::map<uint64_t, Request*> tickets;
+  uint64_t next_ticket = 1;
+  int next_slot = 0;
+  bool stop = false, stop_completer = false;
+  bool use_graph = true;
+  std::thread issuer, completer;
+};
+
+void complete(Engine* e, Request* q, int status, const std::string& err) {
+  std::lock_guard<std::mutex> g(e->mu);
+  q->status = status;
+  q->error = err;
+  q->done = true;
+  e->cv.notify_all();
+}
+
+int slot_graph(Engine* e, Slot& sl) {
+  if (sl.graph || !e->use_graph) return 0;
+  zg_ctx* c = e->c;
+  cudaStream_t cs = nullptr;
+  ZG_CK(cudaStreamCreateWithFlags(&cs, cudaStreamNonBlocking));
+  cudaGraph_t g = nullptr;
+  cudaError_t err = cudaStreamBeginCapture(cs, cudaStreamCaptureModeThreadLocal);
+  int rc = 0;
+  if (err == cudaSuccess) {
+    rc = encode_launches(c, sl.b, 0, true, cs, false);
+    err = cudaStreamEndCapture(cs, &g);
+  }
+  if (err == cudaSuccess && rc == 0) err = cudaGraphInstantiate(&sl.graph, g, 0);
+  if (g) cudaGraphDestroy(g);
+  cudaStreamDestroy(cs);
+  if (err != cudaSuccess || rc) {  // launch the kernels one by one instead
+    cudaGetLastError();
+    sl.graph = nullptr;
+    e->use_graph = false;
+  }
+  return 0;
+}
+
+int issue_encode(Engine* e, int k, Request* q) {
+  zg_ctx* c = e->c;
+  Slot& sl = e->slot[k];
+  const uint8_t* data = q->req.data;
+  const size_t len = q->req.len;
+  zg_reply* r = new zg_reply();
+  q->reply = r;
+  r->slice_size = c->slice_size;
+  r->nslices = 3 * c->R;
+  if (!(r->slices = (uint8_t*)pinned_get(r->nslices * r->slice_size)))
+    return fail(ZG_ERR_CUDA, "cannot allocate pinned reply");
+  if (q->req.require_data) {
+    r->data_len = 3 * c->N * 32;
+    if (!(r->data = (uint8_t*)pinned_get(r->data_len))) return fail(ZG_ERR_CUDA, "cannot allocate pinned reply");
+  }
+  const uint8_t* src = data;
+  cudaPointerAttributes pa;
+  if (len && (cudaPointerGetAttributes(&pa, data) != cudaSuccess || pa.type != cudaMemoryTypeHost)) {
+    cudaGetLastError();
+    memcpy(sl.h_stage, data, len);
+    src = sl.h_stage;
+  }
+  const uint64_t len64 = len;
+  memcpy(sl.h_small, &len64, 8);
+  std::lock_guard<std::mutex> g(c->mu);
+  ZG_CK(cudaSetDevice(c->device));
+  int rc = slot_graph(e, sl);
+  if (rc) return rc;
+  cudaStream_t s = c->stream;
+  ZG_CK(cudaMemcpyAsync(sl.b.d_len, sl.h_small, 8, cudaMemcpyHostToDevice, e->h2d));
+  if (len) ZG_CK(cudaMemcpyAsync(sl.b.raw, src, len, cudaMemcpyHostToDevice, e->h2d));
+  ZG_CK(cudaEventRecord(sl.ev_in, e->h2d));
+  ZG_CK(cudaStreamWaitEvent(s, sl.ev_in, 0));
+  ZG_CK(cudaStreamWaitEvent(s, c->done, 0));
+  if (sl.graph) {
+    ZG_CK(cudaGraphLaunch(sl.graph, s));
+  } else if ((rc = encode_launches(c, sl.b, len, false, s, false))) {
+    return rc;
+  }
+  c->launches += launches_per_encode(c);
+  ZG_CK(cudaEventRecord(c->done, s));
+  ZG_CK(cudaEventRecord(sl.ev_comp, s));
+  ZG_CK(cudaStreamWaitEvent(e->d2h, sl.ev_comp, 0));
+  for (int cs = 0; cs < 3; ++cs)
+    ZG_CK(cudaMemcpyAsync(sl.h_small + 8 + 64 * cs, sl.b.amt + (size_t)cs * (4 * c->R - 2) * 64, 64,
+                          cudaMemcpyDeviceToHost, e->d2h));
+  ZG_CK(cudaMemcpyAsync(sl.h_small + 200, sl.b.tree + c->tree_off[0], 96, cudaMemcpyDeviceToHost, e->d2h));
+  ZG_CK(cudaMemcpyAsync(sl.h_small + 296, sl.b.file_root, 32, cudaMemcpyDeviceToHost, e->d2h));
+  ZG_CK(cudaMemcpyAsync(r->slices, sl.b.slices, r->nslices * r->slice_size, cudaMemcpyDeviceToHost, e->d2h));
+  if (r->data) ZG_CK(cudaMemcpyAsync(r->data, sl.b.enc, r->data_len, cudaMemcpyDeviceToHost, e->d2h));
+  ZG_CK(cudaEventRecord(sl.ev_out, e->d2h));
+  return 0;
+}
+
+// after the slot's copy-out: the reply fields zg_encode fills
+int finish_encode(Engine* e, Slot& sl) {
+  cudaError_t err = cudaEventSynchronize(sl.ev_out);
+  if (err != cudaSuccess) return fail(ZG_ERR_CUDA, std::string("encode: ") + cudaGetErrorString(err));
+  zg_reply* r = sl.req->reply;
+  const uint8_t* amt = sl.h_small + 8;
+  if (memcmp(amt, amt + 64, 64) || memcmp(amt, amt + 128, 64))
+    return fail(ZG_ERR_INTERNAL, "coset commitments differ");
+  if (amt[63] & 0x40) {
+    memset(r->commitment, 0, 64);
+  } else {
+    memcpy(r->commitment, amt, 64);
+    r->commitment[63] &= 0x3f;
+  }
+  memcpy(r->roots, sl.h_small + 200, 96);
+  memcpy(r->storage_root, sl.h_small + 296, 32);
+  return 0;
+}
+
+void issuer_loop(Engine* e) {
+  cudaSetDevice(e->c->device);
+  for (;;) {
+    Request* q = nullptr;
+    int k = -1;
+    {
+      std::unique_lock<std::mutex> lk(e->mu);
+      e->cv.wait(lk, [&] { return e->stop || !e->queue.empty(); });
+      if (e->queue.empty()) break;
+      q = e->queue.front();
+      e->queue.pop_front();
+      if (q->req.kind == ZG_REQ_RECOVER) {
+        e->cv.wait(lk, [&] { return e->inflight.empty(); });
+      } else {
+        k = e->next_slot;
+        e->cv.wait(lk, [&] { return e->slot[k].req == nullptr; });
+        e->slot[k].req = q;
+        e->next_slot ^= 1;
+      }
+    }
+    if (k < 0) {
+      zg_reply* r = new zg_reply();
+      q->reply = r;
+      r->payload.resize(e->c->max_raw);
+      size_t out_len = 0;
+      int rc = zg_recover(e->c, q->req.row_ids, q->req.rows, q->req.row_lens, q->req.n_rows, r->payload.data(),
+                          r->payload.size(), &out_len);
+      if (rc == ZG_OK) r->payload.resize(out_len);
+      complete(e, q, rc, rc ? g_err : std::string());
+      continue;
+    }
+    int rc = issue_encode(e, k, q);
+    if (rc) {
+      // whatever was queued for the slot must end before it is reused
+      cudaStreamSynchronize(e->h2d);
+      cudaStreamSynchronize(e->c->stream);
+      cudaStreamSynchronize(e->d2h);
+      std::string m = g_err;
+      {
+        std::lock_guard<std::mutex> g(e->mu);
+        e->slot[k].req = nullptr;
+      }
+      complete(e, q, rc, m);
+    } else {
+      std::lock_guard<std::mutex> g(e->mu);
+      e->inflight.push_back(k);
+      e->cv.notify_all();
+    }
+  }
+}
+
+void completer_loop(Engine* e) {
+  cudaSetDevice(e->c->device);
+  for (;;) {
+    int k;
+    {
+      std::unique_lock<std::mutex> lk(e->mu);
+      e->cv.wait(lk, [&] { return e->stop_completer || !e->inflight.empty(); });
+      if (e->inflight.empty()) break;
+      k = e->inflight.front();
+    }
+    Slot& sl = e->slot[k];
+    Request* q = sl.req;
+    int rc = finish_encode(e, sl);
+    std::string m = rc ? g_err : std::string();
+    {
+      std::lock_guard<std::mutex> g(e->mu);
+      e->inflight.pop_front();
+      sl.req = nullptr;
+    }
+    complete(e, q, rc, m);
+  }
+}
+
+int engine_start(zg_ctx* c) {
+  std::lock_guard<std::mutex> g(c->eng_mu);
+  if (c->eng) return 0;
+  ZG_CK(cudaSetDevice(c->device));
+  Engine* e = new Engine();
+  e->c = c;
+  auto bail = [&](int rc) {
+    engine_shutdown(e);
+    return rc;
+  };
+  const size_t N = c->N, R = c->R;
+  for (Slot& sl : e->slot) {
+    if (cudaMalloc(&sl.b.raw, c->max_blob + 16) || cudaMalloc(&sl.b.d_len, 8) || cudaMalloc(&sl.b.enc, 3 * N * 32) ||
+        cudaMalloc(&sl.b.tree, c->tree_bytes) || cudaMalloc(&sl.b.amt, 3 * (4 * R - 2) * 64) ||
+        cudaMalloc(&sl.b.slices, 3 * R * c->slice_size) || cudaMalloc(&sl.b.file_root, 32) ||
+        cudaMallocHost(&sl.h_stage, c->max_blob + 16) || cudaMallocHost(&sl.h_small, 512) ||
+        cudaEventCreateWithFlags(&sl.ev_in, cudaEventDisableTiming) ||
+        cudaEventCreateWithFlags(&sl.ev_comp, cudaEventDisableTiming) ||
+        cudaEventCreateWithFlags(&sl.ev_out, cudaEventDisableTiming | cudaEventBlockingSync))
+      return bail(fail(ZG_ERR_CUDA, std::string("pipeline buffers: ") + cudaGetErrorString(cudaGetLastError())));
+  }
+  if (cudaStreamCreateWithFlags(&e->h2d, cudaStreamNonBlocking) ||
+      cudaStreamCreateWithFlags(&e->d2h, cudaStreamNonBlocking))
+    return bail(fail(ZG_ERR_CUDA, "pipeline streams"));
+  e->issuer = std::thread(issuer_loop, e);
+  e->completer = std::thread(completer_loop, e);
+  c->eng = e;
+  return 0;
+}
+
+// Drains the queue and the slots, then frees the pipeline. Requests nobody
+// waited for are freed with their replies.
+void engine_shutdown(Engine* e) {
+  {
+    std::lock_guard<std::mutex> g(e->mu);
+    e->stop = true;
+    e->cv.notify_all();
+  }
+  if (e->issuer.joinable()) e->issuer.join();
+  {
+    std::lock_guard<std::mutex> g(e->mu);
+    e->stop_completer = true;
+    e->cv.notify_all();
+  }
+  if (e->completer.joinable()) e->completer.join();
+  cudaSetDevice(e->c->device);
+  for (auto& kv : e->tickets) {
+    zg_reply_free(kv.second->reply);
+    delete kv.second;
+  }
+  for (Slot& sl : e->slot) {
+    if (sl.ev_out) cudaEventSynchronize(sl.ev_out);
+    if (sl.graph) cudaGraphExecDestroy(sl.graph);
+    void* d[] = {sl.b.raw, sl.b.d_len, sl.b.enc, sl.b.tree, sl.b.amt, sl.b.slices, sl.b.file_root};
+    for (void* p : d) if (p) cudaFree(p);
+    if (sl.h_stage) cudaFreeHost(sl.h_stage);
+    if (sl.h_small) cudaFreeHost(sl.h_small);
+    for (cudaEvent_t ev : {sl.ev_in, sl.ev_comp, sl.ev_out}) if (ev) cudaEventDestroy(ev);
+  }
+  if (e->h2d) cudaStreamDestroy(e->h2d);
+  if (e->d2h) cudaStreamDestroy(e->d2h);
+  e->c->eng = nullptr;
+  delete e;
+}
+
 }  // namespace
 
 extern "C" {
@@ -725,6 +1063,7 @@ int zg_ctx_create(const zg_config* cfg, zg_ctx** out) {
 
 void zg_ctx_destroy(zg_ctx* c) {
   if (!c) return;
+  if (c->eng) engine_shutdown(c->eng);
   cudaSetDevice(c->device);
   if (c->done) cudaEventSynchronize(c->done);  // work queued on caller streams
   if (c->stream) cudaStreamSynchronize(c->stream);
@@ -828,6 +1167,112 @@ int zg_encode(zg_ctx* c, const uint8_t* data, size_t len, int require_data, zg_r
   }
   *out = r;
   return ZG_OK;
+}
+
+int zg_submit(zg_ctx* c, const zg_request* req, uint64_t* ticket) {
+  if (!c || !req || !ticket) return fail(ZG_ERR_INVALID_ARG, "null argument");
+  if (req->kind == ZG_REQ_ENCODE) {
+    if (!req->data && req->len) return fail(ZG_ERR_INVALID_ARG, "null payload");
+    if (req->len > c->max_raw) {  // RawData::try_from (crates/encoder/src/raw_data.rs:76-95)
+      char m[128];
+      snprintf(m, sizeof(m), "TooLargeBlob { actual: %zu, expected_max: %zu }", req->len, c->max_raw);
+      return fail(ZG_ERR_TOO_LARGE_BLOB, m);
+    }
+  } else if (req->kind == ZG_REQ_RECOVER) {
+    if (req->n_rows && (!req->row_ids || !req->rows || !req->row_lens)) return fail(ZG_ERR_INVALID_ARG, "null rows");
+  } else {
+    return fail(ZG_ERR_INVALID_ARG, "unknown request kind");
+  }
+  int rc = engine_start(c);
+  if (rc) return rc;
+  Engine* e = c->eng;
+  Request* q = new Request();
+  q->req = *req;
+  std::lock_guard<std::mutex> g(e->mu);
+  *ticket = e->next_ticket++;
+  e->tickets[*ticket] = q;
+  e->queue.push_back(q);
+  e->cv.notify_all();
+  return ZG_OK;
+}
+
+int zg_wait(zg_ctx* c, uint64_t ticket, int64_t timeout_ms, zg_reply** out) {
+  if (!c || !out) return fail(ZG_ERR_INVALID_ARG, "null argument");
+  *out = nullptr;
+  Engine* e = c->eng;
+  if (!e) return fail(ZG_ERR_INVALID_ARG, "unknown ticket");
+  std::unique_lock<std::mutex> lk(e->mu);
+  auto it = e->tickets.find(ticket);
+  if (it == e->tickets.end()) return fail(ZG_ERR_INVALID_ARG, "unknown ticket");
+  Request* q = it->second;
+  auto ready = [&] { return q->done; };
+  if (timeout_ms < 0) {
+    e->cv.wait(lk, ready);
+  } else if (!e->cv.wait_for(lk, std::chrono::milliseconds(timeout_ms), ready)) {
+    return fail(ZG_ERR_TIMEOUT, "request not finished");
+  }
+  e->tickets.erase(it);
+  lk.unlock();
+  const int status = q->status;
+  if (status == ZG_OK) {
+    *out = q->reply;
+  } else {
+    zg_reply_free(q->reply);
+    fail(status, q->error);
+  }
+  delete q;
+  return status;
+}
+
+int zg_encode_batch(zg_ctx* c, size_t n, const uint8_t* const* data, const size_t* lens, int require_data,
+                    zg_reply** out) {
+  if (!c || (n && (!data || !lens || !out))) return fail(ZG_ERR_INVALID_ARG, "null argument");
+  for (size_t i = 0; i < n; ++i) {
+    out[i] = nullptr;
+    if (!data[i] && lens[i]) return fail(ZG_ERR_INVALID_ARG, "null payload");
+    if (lens[i] > c->max_raw) {
+      char m[160];
+      snprintf(m, sizeof(m), "TooLargeBlob { actual: %zu, expected_max: %zu }", lens[i], c->max_raw);
+      return fail(ZG_ERR_TOO_LARGE_BLOB, m);
+    }
+  }
+  std::vector<uint64_t> t(n);
+  int first = ZG_OK;
+  std::string first_msg;
+  size_t issued = 0;
+  for (; issued < n; ++issued) {
+    zg_request q{};
+    q.kind = ZG_REQ_ENCODE;
+    q.data = data[issued];
+    q.len = lens[issued];
+    q.require_data = require_data;
+    int rc = zg_submit(c, &q, &t[issued]);
+    if (rc) {
+      first = rc;
+      first_msg = g_err;
+      break;
+    }
+  }
+  for (size_t i = 0; i < issued; ++i) {
+    int rc = zg_wait(c, t[i], -1, &out[i]);
+    if (rc && first == ZG_OK) {
+      first = rc;
+      first_msg = g_err;
+    }
+  }
+  if (first != ZG_OK) {
+    for (size_t i = 0; i < n; ++i) {
+      zg_reply_free(out[i]);
+      out[i] = nullptr;
+    }
+    return fail(first, first_msg);
+  }
+  return ZG_OK;
+}
+
+const uint8_t* zg_reply_payload(const zg_reply* r, size_t* len) {
+  if (len) *len = r ? r->payload.size() : 0;
+  return r && !r->payload.empty() ? r->payload.data() : nullptr;
 }
 
 int zg_ctx_warmup(zg_ctx* c) {

@@ -71,10 +71,15 @@ __device__ __forceinline__ Fr pow_split(const Fr* lo, const Fr* hi, uint32_t e, 
 // D[r][j] is the Fr of the 31-byte chunk r*C + j of the zero-padded RawData
 // whose last four bytes hold the payload length (raw_data.rs:55-73,
 // raw_blob.rs:33-40).
-__global__ void __launch_bounds__(256) k_rows_from_raw(const uint8_t* __restrict__ raw, uint64_t len, uint64_t max_raw, int lr, int lc,
-                                uint8_t* __restrict__ enc0, Fr* __restrict__ T1, const Fr* __restrict__ twi_c,
-                                const Fr* __restrict__ wni_lo, const Fr* __restrict__ wni_hi) {
+// The payload length is `len`, or *d_len when d_len is set (graph launches,
+// whose parameters are fixed at capture).
+__global__ void __launch_bounds__(256) k_rows_from_raw(const uint8_t* __restrict__ raw, uint64_t len,
+                                                       const uint64_t* __restrict__ d_len, uint64_t max_raw, int lr,
+                                                       int lc, uint8_t* __restrict__ enc0, Fr* __restrict__ T1,
+                                                       const Fr* __restrict__ twi_c, const Fr* __restrict__ wni_lo,
+                                                       const Fr* __restrict__ wni_hi) {
   extern __shared__ __align__(16) uint8_t smem[];
+  if (d_len) len = *d_len;
   const int C = 1 << lc;
   const uint32_t r = blockIdx.x;
   Fr* s = reinterpret_cast<Fr*>(smem);

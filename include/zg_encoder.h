@@ -32,6 +32,7 @@ extern "C" {
 #define ZG_OK 0
 #define ZG_ERR_TOO_LARGE_BLOB 1
 #define ZG_ERR_RECOVERY 2
+#define ZG_ERR_TIMEOUT 3
 #define ZG_ERR_INVALID_ARG (-1)
 #define ZG_ERR_CUDA (-2)
 #define ZG_ERR_PARAMS (-3)
@@ -117,6 +118,37 @@ int zg_probe_imad(int device, double* gimad_per_s);
  * a value >= r (the reference panics) give their own messages. */
 int zg_recover(zg_ctx* ctx, const uint64_t* row_ids, const uint8_t* const* rows, const size_t* row_lens, size_t n,
                uint8_t* out, size_t out_cap, size_t* out_len);
+
+/* Request pipeline, the serving path (the reference serves EncodeBlob on
+ * tokio workers, grpc/src/service.rs:49-65; recovery is
+ * recover_from_da_slice). zg_submit queues a request and returns at once;
+ * zg_wait blocks for its result (timeout_ms < 0: no limit; ZG_ERR_TIMEOUT
+ * leaves it queued). Requests run in submission order; two blob slots let one
+ * blob's host<->device copies overlap another's compute. The caller keeps
+ * the request's input buffers valid until zg_wait has returned its result.
+ * Encode replies are zg_encode's; recovery replies hold the payload
+ * (zg_reply_payload). A failed request's status comes back from zg_wait with
+ * its message in zg_last_error(). TooLargeBlob is reported by zg_submit. */
+#define ZG_REQ_ENCODE 0
+#define ZG_REQ_RECOVER 1
+typedef struct zg_request {
+  int kind;
+  const uint8_t* data; /* encode */
+  size_t len;
+  int require_data;
+  const uint64_t* row_ids; /* recover: as zg_recover */
+  const uint8_t* const* rows;
+  const size_t* row_lens;
+  size_t n_rows;
+} zg_request;
+int zg_submit(zg_ctx* ctx, const zg_request* req, uint64_t* ticket);
+int zg_wait(zg_ctx* ctx, uint64_t ticket, int64_t timeout_ms, zg_reply** out);
+const uint8_t* zg_reply_payload(const zg_reply* r, size_t* len);
+/* n encodes through the pipeline (uneven payloads welcome); out[i] as
+ * zg_encode's reply for data[i], bit-identical to it. On any error no reply
+ * is returned. */
+int zg_encode_batch(zg_ctx* ctx, size_t n, const uint8_t* const* data, const size_t* lens, int require_data,
+                    zg_reply** out);
 
 /* Kernel-level entry points (device pointers, stream-ordered on `stream`).
  * zg_msm_chunks: the AMT plugin's MSM decomposition (prove_gpu.rs:55-87):

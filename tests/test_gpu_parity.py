@@ -360,6 +360,20 @@ def test_production_recovery_round_trip(prod, gpu_pkg):
         gpu_pkg.recover_from_da_slice(params, bad)
 
 
+def test_production_batch_uneven(prod, gpu_pkg):
+    """Uneven payloads through the pipelined batch path: every reply equals the
+    plain per-blob path's (the full-size payload's reply is the fixture's)."""
+    params, _, payload, reply = prod
+    rng = np.random.default_rng(44)
+    sizes = [65536, 20_000_000, 0]
+    payloads = [payload] + [rng.integers(0, 256, n, dtype=np.uint8).tobytes() for n in sizes]
+    svc = gpu_pkg.EncoderService(params)
+    got = svc.process_batch(payloads, True)
+    assert got[0] == reply
+    for p, g in zip(payloads[1:], got[1:]):
+        assert g == svc.process_data(p, True)
+
+
 def test_encode_matches_golden_fixture(gpu_pkg):
     """The CUDA path against the independent pure-Python restatement's bytes
     (tests/golden/make_golden.py, 8 x 32 blob)."""
