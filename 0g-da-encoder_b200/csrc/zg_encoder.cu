@@ -264,8 +264,9 @@ struct zg_ctx {
 };
 
 // Process-wide pool of page-locked reply buffers: pinning ~200 MB per reply
-// costs far more than the copies themselves, so freed buffers are kept (a few
-// per size) for the next reply.
+// costs far more than the copies themselves, so freed buffers are kept (up to
+// eight per size: two pipeline slots in flight plus replies being consumed)
+// for the next reply.
 namespace {
 std::mutex g_pin_mu;
 std::multimap<size_t, void*> g_pin_pool;
@@ -286,7 +287,7 @@ void* pinned_get(size_t bytes) {
 void pinned_put(void* p, size_t bytes) {
   if (!p) return;
   std::lock_guard<std::mutex> g(g_pin_mu);
-  if (g_pin_pool.count(bytes) < 4) g_pin_pool.emplace(bytes, p);
+  if (g_pin_pool.count(bytes) < 8) g_pin_pool.emplace(bytes, p);
   else cudaFreeHost(p);
 }
 }  // namespace

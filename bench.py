@@ -10,9 +10,18 @@ tau), keccak Merkle tree, and the 3072 serialized EncodedSlices.
   value : blobs/s with the payload already in HBM (zg_encode_device), each
           step timed with CUDA events on the launching stream; L2 is flushed
           between steps (256 MiB write, outside the events)
-  e2e   : blobs/s through zg_encode (EncoderService::process_data) with the
-          payload in pinned host memory: H2D of the payload, the pipeline and
-          the D2H of the full reply (3072 slices + 96 MiB encoded data)
+  e2e   : blobs/s through the C ABI's request pipeline (zg_submit / zg_wait,
+          the serving path behind EncoderService) with the payload in pinned
+          host memory: H2D of the payload, the encode and the D2H of the full
+          reply (3072 slices + 96 MiB encoded data), each reply consumed and
+          freed as it completes; `plain_value` is the same through the
+          blocking per-blob zg_encode (process_data)
+  batched_uneven : blobs/s of the pipelined path over blobs of uneven
+          payload size L ~ U[64 KiB, MAX_RAW_DATA_SIZE] (seeded)
+  serving : Poisson arrivals of requests (payload log-uniform on [4 KiB,
+          MAX_RAW_DATA_SIZE], 10 % recovery requests from 1536 of the 3072
+          rows, each result checked) through the pipeline: completed
+          requests/s and p50 / p99 latency from arrival to result
 
 Multi-GPU: one process per GPU, independent replicas (weak scaling), max of
 the per-rank times. `--impl reference` times the CPU restatement of the
@@ -84,6 +93,11 @@ def parse():
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap.add_argument("--cpu-sample", type=int, default=0, help="chunk groups in the CPU sample (0 = auto)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--batch-blobs", type=int, default=8, help="blobs in the batched-uneven sample")
+    ap.add_argument("--serve-rate", type=float, default=2.0, help="Poisson arrival rate of the serving sample (1/s)")
+    ap.add_argument("--serve-requests", type=int, default=16, help="requests in the serving sample (0 = skip)")
+    ap.add_argument("--serve-plain", action="store_true",
+                    help="also serve the same arrivals through the blocking per-blob path")
     ap.add_argument("--dims", default="10,10",
                     help="LOG_ROW,LOG_COL of the blob; the default 10,10 is the benchmark workload, smaller "
                          "shapes are for profiling captures")
@@ -219,6 +233,130 @@ def reference_arm(args, rank):
     print(json.dumps(out), flush=True)
 
 
+class Pipe:
+    """The C ABI's request pipeline, driven without Python-side reply copies."""
+
+    def __init__(self, pkg, params):
+        self.pkg, self.L, self.h = pkg, pkg.lib(), params.handle
+
+    def _submit(self, q):
+        t = ctypes.c_uint64()
+        rc = self.L.zg_submit(self.h, ctypes.byref(q), ctypes.byref(t))
+        assert rc == 0, self.L.zg_last_error()
+        return t.value
+
+    def submit_encode(self, ptr, n, require_data=1):
+        q = self.pkg._Request()
+        q.kind, q.data, q.len, q.require_data = 0, ptr, n, require_data
+        return self._submit(q)
+
+    def submit_recover(self, rec):
+        ids, bufs, lens, n, _ = rec
+        q = self.pkg._Request()
+        q.kind, q.row_ids, q.rows, q.row_lens, q.n_rows = 1, ids, bufs, lens, n
+        return self._submit(q)
+
+    def wait(self, t):
+        r = ctypes.c_void_p()
+        rc = self.L.zg_wait(self.h, t, -1, ctypes.byref(r))
+        assert rc == 0, self.L.zg_last_error()
+        return r
+
+    def payload(self, r):
+        n = ctypes.c_size_t()
+        p = self.L.zg_reply_payload(r, ctypes.byref(n))
+        return ctypes.string_at(p, n.value) if n.value else b""
+
+    def free(self, r):
+        self.L.zg_reply_free(r)
+
+
+def recovery_inputs(rows, seeds):
+    """ctypes arrays of 1536 of the 3072 rows (seeded erasures), built once."""
+    out = []
+    for sd in seeds:
+        ids = sorted(np.random.default_rng(sd).choice(3 * R, size=3 * R // 2, replace=False).tolist())
+        keep = [rows[i] for i in ids]
+        arr = (ctypes.c_uint64 * len(ids))(*ids)
+        bufs = (ctypes.c_char_p * len(ids))(*keep)
+        lens = (ctypes.c_size_t * len(ids))(*[len(x) for x in keep])
+        out.append((arr, bufs, lens, len(ids), keep))
+    return out
+
+
+def serving_run(pkg, params, pipe, h_ptr, full_payload, recs, rate, n, seed, plain=False):
+    """Poisson arrivals (rate per s) of n requests: 10 % recovery requests (one
+    of `recs`, checked against the original payload), the rest encodes of a
+    payload log-uniform on [4 KiB, MAX_RAW_DATA_SIZE] (a prefix of the pinned
+    payload). Pipeline: a submitter thread submits at each arrival and the
+    caller collects results in order. Plain: one worker serves the arrivals
+    in order through the blocking zg_encode / zg_recover."""
+    import queue
+    import threading
+    rng = np.random.default_rng(seed)
+    gaps = rng.exponential(1.0 / rate, n)
+    arrive = np.cumsum(gaps) - gaps[0]
+    kinds = rng.random(n) < 0.10
+    sizes = np.exp(rng.uniform(np.log(4096), np.log(PAYLOAD), n)).astype(np.int64)
+    which = rng.integers(0, len(recs), n)
+    L = pkg.lib()
+    lat = [0.0] * n
+    bad = []
+    t0 = time.perf_counter() + 0.05
+    if not plain:
+        q = queue.Queue()
+
+        def submitter():
+            for i in range(n):
+                d = t0 + arrive[i] - time.perf_counter()
+                if d > 0:
+                    time.sleep(d)
+                t = pipe.submit_recover(recs[which[i]]) if kinds[i] else pipe.submit_encode(h_ptr, int(sizes[i]))
+                q.put((i, t))
+
+        th = threading.Thread(target=submitter)
+        th.start()
+        for _ in range(n):
+            i, t = q.get()
+            r = pipe.wait(t)
+            done = time.perf_counter()
+            if kinds[i] and pipe.payload(r) != full_payload:
+                bad.append(i)
+            pipe.free(r)
+            lat[i] = done - (t0 + arrive[i])
+        th.join()
+    else:
+        for i in range(n):
+            d = t0 + arrive[i] - time.perf_counter()
+            if d > 0:
+                time.sleep(d)
+            if kinds[i]:
+                ids, bufs, lens, k, _ = recs[which[i]]
+                out = ctypes.create_string_buffer(PAYLOAD)
+                olen = ctypes.c_size_t()
+                rc = L.zg_recover(params.handle, ids, bufs, lens, k, out, PAYLOAD, ctypes.byref(olen))
+                assert rc == 0, L.zg_last_error()
+                if out.raw[:olen.value] != full_payload:
+                    bad.append(i)
+            else:
+                r = ctypes.c_void_p()
+                rc = L.zg_encode(params.handle, ctypes.cast(ctypes.c_void_p(h_ptr), ctypes.c_char_p),
+                                 int(sizes[i]), 1, ctypes.byref(r))
+                assert rc == 0, L.zg_last_error()
+                L.zg_reply_free(r)
+            lat[i] = time.perf_counter() - (t0 + arrive[i])
+    span = max(arrive[i] + lat[i] for i in range(n))
+    lat_ms = np.array(lat) * 1000.0
+    return {
+        "path": "plain per-blob (blocking zg_encode / zg_recover)" if plain else "pipeline (zg_submit / zg_wait)",
+        "arrival_rate_per_s": rate, "requests": n, "recovery_requests": int(kinds.sum()),
+        "completed_per_s": n / span, "p50_ms": float(np.percentile(lat_ms, 50)),
+        "p99_ms": float(np.percentile(lat_ms, 99)), "mean_ms": float(lat_ms.mean()),
+        "payload_mean_bytes": float(sizes[~kinds].mean()) if (~kinds).any() else 0.0,
+        "recovery_mismatches": len(bad),
+    }
+
+
 def main():
     args = parse()
     set_dims(*[int(x) for x in args.dims.split(",")])
@@ -250,14 +388,20 @@ def main():
                                 ctypes.c_void_p(stream.cuda_stream), ctypes.byref(db))
         assert rc == 0, L.zg_last_error()
 
-    def encode_e2e():
+    pipe = Pipe(pkg, params)
+    h_ptr = h_payload.data_ptr()
+
+    def encode_e2e_plain():
         r = ctypes.c_void_p()
-        rc = L.zg_encode(params.handle, ctypes.cast(ctypes.c_void_p(h_payload.data_ptr()), ctypes.c_char_p),
+        rc = L.zg_encode(params.handle, ctypes.cast(ctypes.c_void_p(h_ptr), ctypes.c_char_p),
                          PAYLOAD, 1, ctypes.byref(r))
         assert rc == 0, L.zg_last_error()
-        n = ctypes.c_size_t()
-        L.zg_reply_slice(r, 0, ctypes.byref(n))  # the reply is host-resident after zg_encode returns
-        L.zg_reply_free(r)
+        L.zg_reply_free(r)  # the reply is host-resident once zg_encode returns
+
+    def pipeline(sizes):
+        ts = [pipe.submit_encode(h_ptr, int(n)) for n in sizes]
+        for t in ts:
+            pipe.free(pipe.wait(t))  # the reply is host-resident once zg_wait returns
 
     def barrier():
         torch.cuda.synchronize()
@@ -272,10 +416,12 @@ def main():
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
         return float(t.item())
 
-    # warm-up
+    # warm-up (the pipeline's first blobs also capture its graphs and fill the
+    # pinned reply pool)
     for _ in range(args.warmup):
         encode_device()
-    encode_e2e()
+    encode_e2e_plain()
+    pipeline([PAYLOAD] * max(3, args.warmup))
     torch.cuda.synchronize()
 
     # phase profile (one untimed encode with events between phases)
@@ -311,15 +457,44 @@ def main():
     total_ms = max_over_ranks(total_ms)
     value = world * args.steps / (total_ms / 1000.0)
 
-    # timed: end to end through the public API
+    # timed: end to end through the public API (pipeline), then the blocking path
     barrier()
     t0 = time.perf_counter()
-    for _ in range(args.steps):
-        encode_e2e()
+    pipeline([PAYLOAD] * args.steps)
     torch.cuda.synchronize()
     e2e_s = max_over_ranks(time.perf_counter() - t0)
     barrier()
     e2e_value = world * args.steps / e2e_s
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        encode_e2e_plain()
+    torch.cuda.synchronize()
+    plain_s = max_over_ranks(time.perf_counter() - t0)
+    barrier()
+    e2e_plain = world * args.steps / plain_s
+
+    # batched uneven payloads and a serving sample (single-GPU runs)
+    extra = {}
+    if world == 1 and args.batch_blobs > 0:
+        sizes = np.random.default_rng(4).integers(64 << 10, PAYLOAD + 1, args.batch_blobs)
+        t0 = time.perf_counter()
+        pipeline(sizes)
+        bt = time.perf_counter() - t0
+        extra["batched_uneven"] = {
+            "blobs": int(args.batch_blobs), "value": args.batch_blobs / bt, "unit": UNIT,
+            "payload_mean_bytes": float(sizes.mean()),
+            "path": "pipeline (zg_submit / zg_wait; per-slot CUDA graphs), pinned host payloads, full replies",
+        }
+    if world == 1 and args.serve_requests > 0:
+        rows_reply = pkg.EncoderService(params).process_data(payload.tobytes(), True)
+        rows = [rows_reply.encoded_data[i * (32 << LOG_COL):(i + 1) * (32 << LOG_COL)] for i in range(3 * R)]
+        recs = recovery_inputs(rows, [11, 12, 13])
+        full = payload.tobytes()
+        extra["serving"] = [serving_run(pkg, params, pipe, h_ptr, full, recs, args.serve_rate,
+                                        args.serve_requests, 5)]
+        if args.serve_plain:
+            extra["serving"].append(serving_run(pkg, params, pipe, h_ptr, full, recs, args.serve_rate,
+                                                args.serve_requests, 5, plain=True))
 
     hbm, hbm_tag = measured_peaks()
     t_msm = phases["msm"] / 1000.0
@@ -346,9 +521,12 @@ def main():
         "scaling": "weak", "vs_baseline": None, "dtype": "u32",
         "data": "synthetic (seeded random payload bytes; params from a seeded tau)",
         "config": CONFIG,
-        "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": PAYLOAD, "d2h_bytes_per_step": D2H_BYTES},
+        "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": PAYLOAD, "d2h_bytes_per_step": D2H_BYTES,
+                "path": "zg_submit / zg_wait request pipeline", "plain_value": e2e_plain,
+                "plain_path": "blocking zg_encode per blob"},
         "gpu_launches": launches, "clocks": clk, "roofline": roofline, "phase_rooflines": phase_roofs,
     }
+    out.update(extra)
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         S = args.cpu_sample or auto_sample()
         chunks = cpu_sample_chunks(S)
