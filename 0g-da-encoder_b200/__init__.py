@@ -29,7 +29,7 @@ from . import build as _build
 __all__ = [
     "Dims", "RawData", "EncoderError", "TooLargeBlob", "ZgEncoderParams", "EncodedBlob",
     "EncodeBlobReply", "EncoderService", "lib", "LIB_PATH", "C_ABI_FUNCTIONS", "recover_from_da_slice",
-    "RecoveryError", "Ticket",
+    "RecoveryError", "Ticket", "LightEncodedSlice",
 ]
 
 LIB_PATH = _build.LIB
@@ -76,6 +76,11 @@ class _Request(ctypes.Structure):
 
 
 _SIGS = {
+    "zg_light_slice_from_slice": (ctypes.c_int, [ctypes.c_char_p, _SZ, ctypes.c_uint32, ctypes.c_uint32,
+                                                 ctypes.c_char_p, _SZ, ctypes.POINTER(_SZ)]),
+    "zg_light_slice_into_slice": (ctypes.c_int, [ctypes.c_char_p, _SZ, ctypes.c_char_p, _SZ, ctypes.c_uint32,
+                                                 ctypes.c_uint32, ctypes.c_char_p, _SZ, ctypes.POINTER(_SZ)]),
+    "zg_ctx_msm": (ctypes.c_int, [_P, ctypes.c_uint32, ctypes.c_uint32, _P, _SZ, _P, _P]),
     "zg_submit": (ctypes.c_int, [_P, ctypes.POINTER(_Request), ctypes.POINTER(ctypes.c_uint64)]),
     "zg_wait": (ctypes.c_int, [_P, ctypes.c_uint64, ctypes.c_int64, ctypes.POINTER(_P)]),
     "zg_reply_payload": (_P, [_P, ctypes.POINTER(_SZ)]),
@@ -401,6 +406,36 @@ def recover_from_da_slice(params: ZgEncoderParams, slices: dict) -> bytes:
         raise RecoveryError(L.zg_last_error().decode())
     _check(rc)
     return out.raw[:out_len.value]
+
+
+class LightEncodedSlice:
+    """LightEncodedSlice (crates/encoder/src/encoder/light_slice.rs:11-79) as
+    its ark-serialized bytes: an EncodedSlice without the row."""
+
+    def __init__(self, data: bytes, dims: "Dims" = None):
+        self.data = data
+        self.dims = dims or Dims()
+
+    @classmethod
+    def from_slice(cls, slice_bytes: bytes, dims: "Dims" = None):
+        d = dims or Dims()
+        out = ctypes.create_string_buffer(len(slice_bytes))
+        n = ctypes.c_size_t()
+        _check(lib().zg_light_slice_from_slice(slice_bytes, len(slice_bytes), d.log_row, d.log_col, out, len(out),
+                                               ctypes.byref(n)))
+        return cls(out.raw[:n.value], d)
+
+    @property
+    def index(self) -> int:
+        return int.from_bytes(self.data[:8], "little")
+
+    def into_slice(self, row: bytes) -> bytes:
+        d = self.dims
+        out = ctypes.create_string_buffer(len(self.data) + 32 * d.cols + 40)
+        n = ctypes.c_size_t()
+        _check(lib().zg_light_slice_into_slice(self.data, len(self.data), row, len(row), d.log_row, d.log_col,
+                                               out, len(out), ctypes.byref(n)))
+        return out.raw[:n.value]
 
 
 class EncoderService:

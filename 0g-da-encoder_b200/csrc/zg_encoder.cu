@@ -528,6 +528,7 @@ int encode_launches(zg_ctx* c, const BlobBufs& b, size_t len, bool by_device_len
     fa.lr = lr;
     fa.lc = lc;
     fa.lines = c->L;
+    fa.tabN = N;
     const uint32_t units = (uint32_t)(3 * R * c->L);
     k_fb_accum<<<std::min<unsigned>(c->fb_ctas, units), FB_ACC_THREADS, 0, s>>>(fa, c->fb_gbuf, units);
     mark(3);
@@ -1520,6 +1521,131 @@ int zg_recover(zg_ctx* c, const uint64_t* row_ids, const uint8_t* const* rows, c
   if (out_cap < l32) return fail(ZG_ERR_INVALID_ARG, "output buffer too small");
   memcpy(out, c->h_rec, l32);
   *out_len = l32;
+  return ZG_OK;
+}
+
+int zg_ctx_msm(zg_ctx* c, uint32_t coset, uint32_t line, const void* d_scalars, size_t n, void* d_out, void* stream) {
+  if (!c || !d_scalars || !d_out) return fail(ZG_ERR_INVALID_ARG, "null argument");
+  if (!c->fb) return fail(ZG_ERR_INVALID_ARG, "zg_ctx_msm needs the fixed-base tables (msm_window_bits 0 or 11)");
+  if (coset >= 3 || line >= (uint32_t)c->L) return fail(ZG_ERR_INVALID_ARG, "coset or line out of range");
+  if (n < c->C || n > c->N || (n & (n - 1))) return fail(ZG_ERR_INVALID_ARG, "n must be a power of two in [2^log_col, N]");
+  int lrn = 0;
+  while (((size_t)c->C << lrn) < n) ++lrn;
+  const uint32_t nch = 1u << lrn;
+  std::lock_guard<std::mutex> g(c->mu);
+  ZG_CK(cudaSetDevice(c->device));
+  cudaStream_t s = (cudaStream_t)stream;
+  ZG_CK(cudaStreamWaitEvent(s, c->done, 0));
+  k_fb_sort<<<dim3(nch, 1), 256, fb_sort_smem_bytes(c->lc), s>>>((const uint8_t*)d_scalars, c->fb_offs, c->fb_ents,
+                                                                  lrn, c->lc, 0, 0);
+  FbAccArgs fa;
+  fa.tab = c->line_ptr((int)coset, (int)line);
+  fa.offs = c->fb_offs;
+  fa.ents = c->fb_ents;
+  fa.outT = c->fb_T;
+  fa.outS = c->fb_S;
+  fa.lr = lrn;
+  fa.lc = c->lc;
+  fa.lines = 1;
+  fa.tabN = c->N;
+  k_fb_accum<<<std::min<unsigned>(c->fb_ctas, nch), FB_ACC_THREADS, 0, s>>>(fa, c->fb_gbuf, nch);
+  k_fb_combine<<<nblk(nch, 64), 64, 0, s>>>(c->fb_T, c->fb_S, c->part, lrn, 1, nch);
+  k_sum_points<<<1, 256, 0, s>>>(c->part, nch, c->nodes);
+  k_serialize_nodes<<<1, 128, 0, s>>>(c->nodes, (uint8_t*)d_out, 1);
+  c->launches += 5;
+  ZG_CK(cudaEventRecord(c->done, s));
+  return check_launch();
+}
+
+// ---- LightEncodedSlice (crates/encoder/src/encoder/light_slice.rs:11-79):
+// the ark-serialized slice without its row. Both layouts are fixed-offset:
+//   EncodedSlice: index | amt.index | commitment | row.index | (len, row) |
+//                 (len, proof pairs) | high | roots | (len, path) | merkle.index | leaf
+//   Light:        index | commitment | (len, proof pairs) | high | roots | (len, path) | leaf
+namespace {
+struct SliceLayout {
+  size_t C, lr, row, proof, high, roots, path, midx, leaf, size, light_size;
+  SliceLayout(uint32_t log_row, uint32_t log_col) {
+    C = size_t(1) << log_col;
+    lr = log_row;
+    row = 88;
+    proof = 96 + 32 * C;
+    high = proof + 8 + 128 * lr;
+    roots = high + 64;
+    path = roots + 96;
+    midx = path + 8 + 32 * lr;
+    leaf = midx + 8;
+    size = leaf + 32;
+    light_size = 8 + 64 + (8 + 128 * lr) + 64 + 96 + (8 + 32 * lr) + 32;
+  }
+};
+uint64_t get_u64(const uint8_t* p) {
+  uint64_t v;
+  memcpy(&v, p, 8);
+  return v;
+}
+}  // namespace
+
+int zg_light_slice_from_slice(const uint8_t* slice, size_t len, uint32_t log_row, uint32_t log_col, uint8_t* out,
+                              size_t cap, size_t* out_len) {
+  if (!slice || !out || !out_len || log_row < 1 || log_row > 20 || log_col > 20)
+    return fail(ZG_ERR_INVALID_ARG, "bad arguments");
+  const SliceLayout L(log_row, log_col);
+  if (len != L.size) return fail(ZG_ERR_INVALID_ARG, "slice length does not match the blob shape");
+  if (get_u64(slice + L.row) != L.C || get_u64(slice + L.proof) != L.lr || get_u64(slice + L.path) != L.lr)
+    return fail(ZG_ERR_INVALID_ARG, "slice vector lengths do not match the blob shape");
+  const uint64_t index = get_u64(slice);
+  char m[160];
+  // EncodedSlice::check_amt_idx / check_merkle_idx (slice.rs:41-71), unwrapped by from_slice
+  if (get_u64(slice + 8) != index) {
+    snprintf(m, sizeof(m), "UnmatchedAMTIndex { row_index: %llu, amt_index: %llu }", (unsigned long long)index,
+             (unsigned long long)get_u64(slice + 8));
+    return fail(ZG_ERR_INVALID_ARG, m);
+  }
+  if (get_u64(slice + L.midx) != index) {
+    snprintf(m, sizeof(m), "UnmatchedMerkleIndex { row_index: %llu, merkle_index: %llu }",
+             (unsigned long long)index, (unsigned long long)get_u64(slice + L.midx));
+    return fail(ZG_ERR_INVALID_ARG, m);
+  }
+  if (cap < L.light_size) return fail(ZG_ERR_INVALID_ARG, "output buffer too small");
+  uint8_t* o = out;
+  memcpy(o, slice, 8), o += 8;
+  memcpy(o, slice + 16, 64), o += 64;
+  memcpy(o, slice + L.proof, L.roots - L.proof), o += L.roots - L.proof;  // proof pairs, high
+  memcpy(o, slice + L.roots, L.midx - L.roots), o += L.midx - L.roots;    // roots, path
+  memcpy(o, slice + L.leaf, 32), o += 32;
+  *out_len = L.light_size;
+  return ZG_OK;
+}
+
+int zg_light_slice_into_slice(const uint8_t* light, size_t len, const uint8_t* row, size_t row_len,
+                              uint32_t log_row, uint32_t log_col, uint8_t* out, size_t cap, size_t* out_len) {
+  if (!light || !row || !out || !out_len || log_row < 1 || log_row > 20 || log_col > 20)
+    return fail(ZG_ERR_INVALID_ARG, "bad arguments");
+  const SliceLayout L(log_row, log_col);
+  if (len != L.light_size) return fail(ZG_ERR_INVALID_ARG, "light slice length does not match the blob shape");
+  if (row_len != 32 * L.C) return fail(ZG_ERR_INVALID_ARG, "row length does not match the blob shape");
+  if (cap < L.size) return fail(ZG_ERR_INVALID_ARG, "output buffer too small");
+  const uint64_t index = get_u64(light);
+  const uint64_t R = uint64_t(1) << log_row;
+  const uint8_t* proof = light + 72;
+  const size_t proof_bytes = L.roots - L.proof;  // (len, pairs) and high
+  const uint8_t* roots = proof + proof_bytes;
+  const size_t roots_bytes = L.midx - L.roots;   // roots and (len, path)
+  const uint8_t* leaf = roots + roots_bytes;
+  uint8_t* o = out;
+  auto put = [&](uint64_t v) { memcpy(o, &v, 8), o += 8; };
+  put(index);
+  put(index);                   // EncodedSliceAMT::new(self.index, ...)
+  memcpy(o, light + 8, 64), o += 64;
+  put(index % R);               // BlobRow.index
+  put(L.C);
+  memcpy(o, row, 32 * L.C), o += 32 * L.C;
+  memcpy(o, proof, proof_bytes), o += proof_bytes;
+  memcpy(o, roots, roots_bytes), o += roots_bytes;
+  put(index);                   // EncodedSliceMerkle::new(..., self.index, ...)
+  memcpy(o, leaf, 32), o += 32;
+  *out_len = L.size;
   return ZG_OK;
 }
 

@@ -489,12 +489,13 @@ __global__ void __launch_bounds__(256) k_fb_sort(const uint8_t* __restrict__ sca
 }
 
 struct FbAccArgs {
-  const G1Aff* tab;     // [cosets][lines][W][N]
+  const G1Aff* tab;     // [cosets][lines][W][tabN]
   const uint32_t* offs;
   const uint16_t* ents;
   XYZZ* outT;           // [cosets * nchunks * lines][FB_ACC_THREADS]
   XYZZ* outS;
-  int lr, lc, lines;
+  int lr, lc, lines;    // 2^lr chunks of 2^lc points per coset
+  uint64_t tabN;        // points per window table (the param line length)
 };
 
 // Persistent CTAs over the (chunk, line) work items. Per item:
@@ -517,7 +518,7 @@ __global__ void __launch_bounds__(FB_ACC_THREADS, 4) k_fb_accum(FbAccArgs a, XYZ
   __shared__ uint32_t bins[FB_TASK + 1];
   XYZZ* gpart = gpart_all + (size_t)blockIdx.x * FB_MAX_TASKS;
   const uint32_t nch = 1u << a.lr;
-  const uint64_t N = 1ull << (a.lr + a.lc);
+  const uint64_t N = a.tabN;
   for (uint32_t u = blockIdx.x; u < units; u += gridDim.x) {
     const uint32_t l = u % a.lines, g = u / a.lines;
     const uint32_t coset = g / nch, b = g % nch;
@@ -625,6 +626,24 @@ __global__ void __launch_bounds__(64) k_fb_combine(const XYZZ* __restrict__ T, c
   for (int k = 0; k < 3; ++k) wsum = wsum.dbl();  // x FB_PER_THREAD = 8
   tot.add(wsum);
   store_xyzz(part + ((size_t)coset * lines + l) * nch + b, tot);
+}
+
+// out = sum of the n points of `in` (one CTA of 256 threads)
+__global__ void __launch_bounds__(256) k_sum_points(const XYZZ* __restrict__ in, uint32_t n, XYZZ* __restrict__ out) {
+  __shared__ XYZZ sh[256];
+  XYZZ acc = XYZZ::inf();
+  for (uint32_t i = threadIdx.x; i < n; i += blockDim.x) acc.add(load_xyzz(in + i));
+  sh[threadIdx.x] = acc;
+  __syncthreads();
+  for (int w = 128; w > 0; w >>= 1) {
+    if ((int)threadIdx.x < w) {
+      XYZZ t = sh[threadIdx.x];
+      t.add(sh[threadIdx.x + w]);
+      sh[threadIdx.x] = t;
+    }
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) store_xyzz(out, sh[0]);
 }
 
 // sum_w 2^{8w} win[w] for each (coset, line, chunk)

@@ -98,6 +98,10 @@ def parse():
     ap.add_argument("--serve-requests", type=int, default=16, help="requests in the serving sample (0 = skip)")
     ap.add_argument("--serve-plain", action="store_true",
                     help="also serve the same arrivals through the blocking per-blob path")
+    ap.add_argument("--micro", action="store_true",
+                    help="kernel microbenchmarks instead of the blob benchmark: single MSMs of 2^16/2^18/2^20 "
+                         "points (uniform and blob-like scalars), NTTs (1024 x 2^10, 64 x 2^14, 1 x 2^20; "
+                         "forward, inverse, coset), Keccak Merkle over 3072 x 1024 x 32 B")
     ap.add_argument("--dims", default="10,10",
                     help="LOG_ROW,LOG_COL of the blob; the default 10,10 is the benchmark workload, smaller "
                          "shapes are for profiling captures")
@@ -171,6 +175,40 @@ class ClockSampler:
                     reasons.add(name)
         return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
                 "reasons": sorted(reasons), "samples": len(sm)}
+
+
+class Ranks:
+    """Barrier and max-over-ranks around the timed regions (one process per
+    GPU over NCCL; gloo and CPU tensors in the multi-rank tests). Every rank
+    takes the same collective steps in the same order."""
+
+    def __init__(self, dist, device):
+        self.dist, self.device = dist, device
+
+    def _sync(self):
+        if self.device == "cuda":
+            import torch
+            torch.cuda.synchronize()
+
+    def barrier(self):
+        self._sync()
+        if self.dist is not None:
+            self.dist.barrier()
+        self._sync()
+
+    def max(self, x):
+        if self.dist is None:
+            return x
+        import torch
+        t = torch.tensor([x], dtype=torch.float64, device=self.device)
+        self.dist.all_reduce(t, op=self.dist.ReduceOp.MAX)
+        return float(t.item())
+
+
+def job_value(world, steps, max_seconds):
+    """Whole-job throughput: every rank processed `steps` blobs; the job took
+    the slowest rank's time."""
+    return world * steps / max_seconds
 
 
 def dist_setup():
@@ -357,10 +395,111 @@ def serving_run(pkg, params, pipe, h_ptr, full_payload, recs, rate, n, seed, pla
     }
 
 
+def micro(args):
+    """Kernel microbenchmarks on one GPU, one JSON line. Each case: 3 warm-up
+    calls, then `steps` calls timed one by one with CUDA events on the
+    launching stream, L2 flushed (256 MiB write) between calls outside the
+    events; the median is reported."""
+    import torch
+    pkg = load_pkg()
+    L = pkg.lib()
+    params = pkg.ZgEncoderParams.from_seed(LOG_ROW, LOG_COL, PARAM_SEED)
+    stream = torch.cuda.Stream()
+    torch.cuda.set_stream(stream)
+    flush = torch.empty(256 << 20, dtype=torch.uint8, device="cuda")
+    gen = torch.Generator(device="cuda")
+    gen.manual_seed(1234)
+    hbm, hbm_tag = measured_peaks()
+    steps = max(3, args.steps)
+
+    def timed(fn):
+        for _ in range(3):
+            fn()
+        ts = []
+        for k in range(steps):
+            flush.fill_(k & 0xff)
+            a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            a.record(stream)
+            fn()
+            b.record(stream)
+            b.synchronize()
+            ts.append(a.elapsed_time(b))
+        return statistics.median(ts)
+
+    def rand_bytes(n):
+        return torch.randint(0, 256, (n,), dtype=torch.uint8, device="cuda", generator=gen)
+
+    out = {"msm": [], "ntt": [], "keccak_merkle": None}
+    d_out = torch.empty(64, dtype=torch.uint8, device="cuda")
+    basis_line = LOG_ROW  # lines: quotients 0..LOG_ROW-1, basis, high basis
+    rng = np.random.default_rng(3)
+    for logn in (16, 18, 20):
+        n = 1 << logn
+        for kind in ("uniform", "blob"):
+            sc = rand_bytes(32 * n).view(n, 32)
+            z = 0.0
+            if kind == "uniform":
+                sc[:, 31] &= 0x1f  # below 2^253 < r
+            else:  # 31-byte scalars (< 2^248), zero suffix of a fraction z ~ U[0, 0.9]
+                z = float(rng.uniform(0, 0.9))
+                sc[:, 31] = 0
+                sc[int(np.ceil((1 - z) * n)):] = 0
+            sc = sc.contiguous()
+
+            def run():
+                rc = L.zg_ctx_msm(params.handle, 0, basis_line, ctypes.c_void_p(sc.data_ptr()), n,
+                                  ctypes.c_void_p(d_out.data_ptr()), ctypes.c_void_p(stream.cuda_stream))
+                assert rc == 0, L.zg_last_error()
+
+            ms = timed(run)
+            nz = int((1 - z) * n) if kind == "blob" else n
+            out["msm"].append({"points": n, "scalars": kind, "zero_fraction": round(z, 3), "ms": ms,
+                               "points_per_s": n / (ms / 1000.0), "nonzero_points_per_s": nz / (ms / 1000.0)})
+    for batch, logn in ((1024, 10), (64, 14), (1, 20)):
+        n = 1 << logn
+        for mode, inv, coset in (("forward", 0, 0), ("inverse", 1, 0), ("coset1", 0, 1)):
+            v = rand_bytes(32 * n * batch).view(n * batch, 32)
+            v[:, 31] &= 0x2f  # canonical: below r
+
+            def run():
+                rc = L.zg_ntt(ctypes.c_void_p(v.data_ptr()), logn, batch, inv, coset,
+                              ctypes.c_void_p(stream.cuda_stream))
+                assert rc == 0, L.zg_last_error()
+
+            ms = timed(run)
+            byts = 2 * n * batch * 32
+            out["ntt"].append({"batch": batch, "log_n": logn, "mode": mode, "ms": ms,
+                               "algorithmic_bytes": byts, "achieved_gbs": byts / (ms / 1000) / 1e9,
+                               "hbm_frac": byts / (ms / 1000) / 1e9 / hbm,
+                               "butterfly_mul_per_s": batch * (n // 2) * logn / (ms / 1000)})
+    items = rand_bytes(3 * N * 32)
+    roots = torch.empty(96, dtype=torch.uint8, device="cuda")
+
+    def run():
+        rc = L.zg_merkle_roots(ctypes.c_void_p(items.data_ptr()), 3 * N, ctypes.c_void_p(roots.data_ptr()),
+                               ctypes.c_void_p(stream.cuda_stream))
+        assert rc == 0, L.zg_last_error()
+
+    ms = timed(run)
+    out["keccak_merkle"] = {"rows": 3 * R, "row_bytes": 32 << LOG_COL, "ms": ms,
+                            "algorithmic_bytes": MERKLE_BYTES,
+                            "achieved_gbs": MERKLE_BYTES / (ms / 1000) / 1e9,
+                            "hbm_frac": MERKLE_BYTES / (ms / 1000) / 1e9 / hbm,
+                            "keccak_f_per_s": (3 * N // 8 * 2 + 3 * N // 8 - 3) / (ms / 1000)}
+    res = {"micro": out, "imad_probe_gimad_s": pkg.probe_imad(0), "hbm_peak_gbs": hbm, "hbm_peak_src": hbm_tag,
+           "timing": f"median of {steps} calls, CUDA events on the launching stream, L2 flushed between calls",
+           "params": "seeded tau (seed 2024), 1024 x 1024, MSM bases = coset-0 basis line"}
+    print(json.dumps(res), flush=True)
+    params.close()
+
+
 def main():
     args = parse()
     set_dims(*[int(x) for x in args.dims.split(",")])
     rank, world, local = dist_setup()
+    if args.micro:
+        micro(args)
+        return
     if args.impl == "reference":
         reference_arm(args, rank)
         return
@@ -403,18 +542,8 @@ def main():
         for t in ts:
             pipe.free(pipe.wait(t))  # the reply is host-resident once zg_wait returns
 
-    def barrier():
-        torch.cuda.synchronize()
-        if dist is not None:
-            dist.barrier()
-        torch.cuda.synchronize()
-
-    def max_over_ranks(x):
-        if dist is None:
-            return x
-        t = torch.tensor([x], dtype=torch.float64, device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        return float(t.item())
+    ranks = Ranks(dist, "cuda")
+    barrier, max_over_ranks = ranks.barrier, ranks.max
 
     # warm-up (the pipeline's first blobs also capture its graphs and fill the
     # pinned reply pool)
@@ -455,7 +584,7 @@ def main():
     barrier()
     total_ms = sum(s.elapsed_time(e) for s, e in zip(starts, ends))
     total_ms = max_over_ranks(total_ms)
-    value = world * args.steps / (total_ms / 1000.0)
+    value = job_value(world, args.steps, total_ms / 1000.0)
 
     # timed: end to end through the public API (pipeline), then the blocking path
     barrier()
@@ -464,14 +593,14 @@ def main():
     torch.cuda.synchronize()
     e2e_s = max_over_ranks(time.perf_counter() - t0)
     barrier()
-    e2e_value = world * args.steps / e2e_s
+    e2e_value = job_value(world, args.steps, e2e_s)
     t0 = time.perf_counter()
     for _ in range(args.steps):
         encode_e2e_plain()
     torch.cuda.synchronize()
     plain_s = max_over_ranks(time.perf_counter() - t0)
     barrier()
-    e2e_plain = world * args.steps / plain_s
+    e2e_plain = job_value(world, args.steps, plain_s)
 
     # batched uneven payloads and a serving sample (single-GPU runs)
     extra = {}

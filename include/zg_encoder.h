@@ -150,6 +150,26 @@ const uint8_t* zg_reply_payload(const zg_reply* r, size_t* len);
 int zg_encode_batch(zg_ctx* ctx, size_t n, const uint8_t* const* data, const size_t* lens, int require_data,
                     zg_reply** out);
 
+/* One MSM over the first n points of a param line with the context's
+ * fixed-base tables: out = sum_i scalars[i] * line[i], written as a 64-byte
+ * ark G1 (the shape of VariableBaseMSM::msm in prove.rs:17-31 against
+ * `basis`, line log_row, or another line). scalars: n canonical 32-byte Fr
+ * in device memory; n a power of two in [2^log_col, 2^(log_row+log_col)].
+ * Stream-ordered on `stream`, after any earlier encode of the context. */
+int zg_ctx_msm(zg_ctx* ctx, uint32_t coset, uint32_t line, const void* d_scalars, size_t n, void* d_out,
+               void* stream);
+
+/* LightEncodedSlice (crates/encoder/src/encoder/light_slice.rs:11-79), host
+ * byte conversions of the ark-serialized layouts (no device work).
+ * from_slice: LightEncodedSlice::from_slice / EncodedSlice::into_light_slice;
+ * the reference unwraps check_amt_idx / check_merkle_idx, here those come
+ * back as ZG_ERR_INVALID_ARG with the VerifierError text. into_slice:
+ * LightEncodedSlice::into_slice(row), row = C canonical 32-byte scalars. */
+int zg_light_slice_from_slice(const uint8_t* slice, size_t len, uint32_t log_row, uint32_t log_col, uint8_t* out,
+                              size_t cap, size_t* out_len);
+int zg_light_slice_into_slice(const uint8_t* light, size_t len, const uint8_t* row, size_t row_len,
+                              uint32_t log_row, uint32_t log_col, uint8_t* out, size_t cap, size_t* out_len);
+
 /* Kernel-level entry points (device pointers, stream-ordered on `stream`).
  * zg_msm_chunks: the AMT plugin's MSM decomposition (prove_gpu.rs:55-87):
  * for every line l < lines and chunk b < nchunks,

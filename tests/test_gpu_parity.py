@@ -112,6 +112,50 @@ def test_msm_chunks_matches_oracle(gpu_pkg, oracle, small_params_mont):
             assert got[(l * 16 + b) * 64:(l * 16 + b + 1) * 64] == exp, (l, b)
 
 
+@pytest.fixture(scope="module")
+def ctx_4x6(gpu_pkg):
+    params = gpu_pkg.ZgEncoderParams.from_seed(4, 6, 7)
+    yield params
+    params.close()
+
+
+@pytest.mark.parametrize("n,coset,line,kind", [
+    (64, 0, 4, "uniform"), (256, 1, 0, "uniform"), (1024, 0, 4, "uniform"), (1024, 2, 5, "blob"),
+    (512, 0, 3, "edges"), (1024, 1, 4, "zero"),
+])
+def test_ctx_msm_matches_oracle(gpu_pkg, oracle, ctx_4x6, n, coset, line, kind):
+    """zg_ctx_msm: one MSM over the first n points of a param line (fixed-base
+    tables) against the oracle's Pippenger on the same points."""
+    rng = np.random.default_rng(n + 7 * coset + line)
+    if kind == "zero":
+        scal = bytes(32 * n)
+    elif kind == "blob":  # 31-byte scalars with a zero suffix (60 % of the points)
+        b = np.zeros((n, 32), dtype=np.uint8)
+        k = int(n * 0.4)
+        b[:k, :31] = rng.integers(0, 256, size=(k, 31), dtype=np.uint8)
+        scal = b.tobytes()
+    else:
+        scal = bytearray(rand_fr_bytes(rng, n))
+        if kind == "edges":
+            for i, v in enumerate([0, 1, R_MOD - 1, 2, R_MOD - 2, 1 << 252, (1 << 248) - 1]):
+                scal[32 * i:32 * i + 32] = v.to_bytes(32, "little")
+        scal = bytes(scal)
+    bases = ctx_4x6.param_line(coset, line, 0, n)
+    out = empty(64)
+    ts = dev(scal)
+    rc = gpu_pkg.lib().zg_ctx_msm(ctx_4x6.handle, coset, line, ts.data_ptr(), n, out.data_ptr(), None)
+    assert rc == 0, gpu_pkg.lib().zg_last_error()
+    assert host(out) == oracle.msm(bases, scal)
+
+
+def test_ctx_msm_rejects_bad_sizes(gpu_pkg, ctx_4x6):
+    out = empty(64)
+    ts = dev(bytes(32 * 2048))
+    L = gpu_pkg.lib()
+    for n, coset, line in [(32, 0, 0), (96, 0, 0), (2048, 0, 0), (64, 3, 0), (64, 0, 6)]:
+        assert L.zg_ctx_msm(ctx_4x6.handle, coset, line, ts.data_ptr(), n, out.data_ptr(), None) != 0
+
+
 def test_msm_special_cases(gpu_pkg, oracle, small_params_mont):
     """Doubling and cancellation inside buckets: repeated and negated bases."""
     line = mont_lines(small_params_mont[0], 4, 6)[0]
