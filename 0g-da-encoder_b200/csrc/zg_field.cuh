@@ -347,97 +347,6 @@ struct Fp {
   }
 #endif
 
-  // same as mul with the modulus limbs as instruction immediates (diagnostic)
-  ZG_HD static Fp mul_imm(const Fp& a, const Fp& b) {
-#ifdef __CUDA_ARCH__
-    uint32_t t0 = 0, t1 = 0, t2 = 0, t3 = 0, t4 = 0, t5 = 0, t6 = 0, t7 = 0, t8;
-#pragma unroll
-    for (int i = 0; i < 8; ++i) {
-      const uint32_t bi = b.v[i];
-      // t[0..8] = t[0..7] + a * bi   (even limbs chain, then odd limbs chain)
-      asm("mad.lo.cc.u32 %0, %9, %17, %0;\n\t"
-          "madc.hi.cc.u32 %1, %9, %17, %1;\n\t"
-          "madc.lo.cc.u32 %2, %11, %17, %2;\n\t"
-          "madc.hi.cc.u32 %3, %11, %17, %3;\n\t"
-          "madc.lo.cc.u32 %4, %13, %17, %4;\n\t"
-          "madc.hi.cc.u32 %5, %13, %17, %5;\n\t"
-          "madc.lo.cc.u32 %6, %15, %17, %6;\n\t"
-          "madc.hi.cc.u32 %7, %15, %17, %7;\n\t"
-          "addc.u32 %8, 0, 0;\n\t"
-          "mad.lo.cc.u32 %1, %10, %17, %1;\n\t"
-          "madc.hi.cc.u32 %2, %10, %17, %2;\n\t"
-          "madc.lo.cc.u32 %3, %12, %17, %3;\n\t"
-          "madc.hi.cc.u32 %4, %12, %17, %4;\n\t"
-          "madc.lo.cc.u32 %5, %14, %17, %5;\n\t"
-          "madc.hi.cc.u32 %6, %14, %17, %6;\n\t"
-          "madc.lo.cc.u32 %7, %16, %17, %7;\n\t"
-          "madc.hi.u32 %8, %16, %17, %8;"
-          : "+r"(t0), "+r"(t1), "+r"(t2), "+r"(t3), "+r"(t4), "+r"(t5), "+r"(t6), "+r"(t7), "=&r"(t8)
-          : "r"(a.v[0]), "r"(a.v[1]), "r"(a.v[2]), "r"(a.v[3]), "r"(a.v[4]), "r"(a.v[5]), "r"(a.v[6]),
-            "r"(a.v[7]), "r"(bi));
-      const uint32_t m = t0 * C::inv;
-      // t[0..8] += m * p ; t0 becomes 0 and is dropped by the shift below
-      asm("mad.lo.cc.u32 %0, %9, %10, %0;\n\t"
-          "madc.hi.cc.u32 %1, %9, %10, %1;\n\t"
-          "madc.lo.cc.u32 %2, %9, %12, %2;\n\t"
-          "madc.hi.cc.u32 %3, %9, %12, %3;\n\t"
-          "madc.lo.cc.u32 %4, %9, %14, %4;\n\t"
-          "madc.hi.cc.u32 %5, %9, %14, %5;\n\t"
-          "madc.lo.cc.u32 %6, %9, %16, %6;\n\t"
-          "madc.hi.cc.u32 %7, %9, %16, %7;\n\t"
-          "addc.u32 %8, %8, 0;\n\t"
-          "mad.lo.cc.u32 %1, %9, %11, %1;\n\t"
-          "madc.hi.cc.u32 %2, %9, %11, %2;\n\t"
-          "madc.lo.cc.u32 %3, %9, %13, %3;\n\t"
-          "madc.hi.cc.u32 %4, %9, %13, %4;\n\t"
-          "madc.lo.cc.u32 %5, %9, %15, %5;\n\t"
-          "madc.hi.cc.u32 %6, %9, %15, %6;\n\t"
-          "madc.lo.cc.u32 %7, %9, %17, %7;\n\t"
-          "madc.hi.u32 %8, %9, %17, %8;"
-          : "+r"(t0), "+r"(t1), "+r"(t2), "+r"(t3), "+r"(t4), "+r"(t5), "+r"(t6), "+r"(t7), "+r"(t8)
-          : "r"(m), "n"(C::p0), "n"(C::p1), "n"(C::p2), "n"(C::p3), "n"(C::p4), "n"(C::p5), "n"(C::p6),
-            "n"(C::p7));
-      t0 = t1; t1 = t2; t2 = t3; t3 = t4; t4 = t5; t5 = t6; t6 = t7; t7 = t8;
-    }
-    Fp r;
-    r.v[0] = t0; r.v[1] = t1; r.v[2] = t2; r.v[3] = t3;
-    r.v[4] = t4; r.v[5] = t5; r.v[6] = t6; r.v[7] = t7;
-    Fp s;
-    uint32_t borrow = sub_raw(s, r, modulus());
-    return borrow ? r : s;
-#else
-    uint32_t t[10] = {0, 0, 0, 0, 0, 0, 0, 0, 0, 0};
-    const Fp p = modulus();
-    for (int i = 0; i < 8; ++i) {
-      uint64_t c = 0;
-      for (int j = 0; j < 8; ++j) {
-        uint64_t s = (uint64_t)a.v[j] * b.v[i] + t[j] + c;
-        t[j] = (uint32_t)s;
-        c = s >> 32;
-      }
-      uint64_t s = (uint64_t)t[8] + c;
-      t[8] = (uint32_t)s;
-      t[9] = (uint32_t)(s >> 32);
-      uint32_t m = t[0] * C::inv;
-      s = (uint64_t)m * p.v[0] + t[0];
-      c = s >> 32;
-      for (int j = 1; j < 8; ++j) {
-        s = (uint64_t)m * p.v[j] + t[j] + c;
-        t[j - 1] = (uint32_t)s;
-        c = s >> 32;
-      }
-      s = (uint64_t)t[8] + c;
-      t[7] = (uint32_t)s;
-      t[8] = t[9] + (uint32_t)(s >> 32);
-    }
-    Fp r;
-    for (int i = 0; i < 8; ++i) r.v[i] = t[i];
-    Fp d;
-    uint32_t borrow = sub_raw(d, r, p);
-    return (t[8] == 0 && borrow) ? r : d;
-#endif
-  }
-
   // canonical (< p) -> Montgomery
   ZG_HD static Fp from_canonical(const Fp& a) { return mul(a, r2()); }
   // Montgomery -> canonical

@@ -208,7 +208,7 @@ int zg_merkle_roots(const void* d_items, size_t n_items, void* d_roots, void* st
 /* Device arithmetic self test (no reference counterpart): compares the device
  * field and curve routines against the host build of the same code on fixed
  * pseudo-random inputs; fails[k] receives the mismatch count of check k
- * (0 Fq mul, 1 Fq mul with immediate modulus, 2 Fq add, 3 Fq sub, 4 Fr mul,
+ * (0 Fq mul, 1 Fq mul on the FP64 pipe, 2 Fq add, 3 Fq sub, 4 Fr mul,
  * 5 Fr Montgomery round trip, 6 XYZZ add(P, P) == dbl(P)). */
 int zg_selftest(int* fails, int nops);
 

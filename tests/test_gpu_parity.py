@@ -62,6 +62,14 @@ def mont_lines(mont: bytes, log_row, log_col):
 
 
 # ---------------------------------------------------------------------------
+def test_device_arithmetic_selftest(gpu_pkg):
+    """Device field / curve routines against their host build, incl. the
+    FP64-pipe Fq product the MSM pairs with the integer one."""
+    fails = gpu_pkg.selftest()
+    assert fails == {k: 0 for k in fails}, fails
+    assert "fq_mul_f64" in fails
+
+
 @pytest.mark.parametrize("log_n,batch,inverse,coset", [
     (5, 4, 0, 0), (5, 4, 1, 0), (5, 3, 0, 1), (10, 8, 0, 0), (10, 8, 1, 0), (10, 2, 0, 2),
     (11, 2, 1, 0), (14, 1, 0, 0), (14, 1, 1, 0), (20, 1, 0, 1), (20, 1, 1, 0),
