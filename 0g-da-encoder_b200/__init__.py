@@ -65,6 +65,21 @@ class _DeviceBlob(ctypes.Structure):
     ]
 
 
+class _Tuning(ctypes.Structure):
+    """zg_tuning (include/zg_encoder.h)."""
+    _fields_ = [("msm_product", ctypes.c_uint32), ("ntt_cols_per_cta", ctypes.c_uint32),
+                ("ntt_threads", ctypes.c_uint32), ("msm_ms", ctypes.c_float * 3), ("ntt_ms", ctypes.c_float * 9)]
+
+
+MSM_PRODUCTS = ("imad", "hybrid", "fp64")  # ZG_MSM_PRODUCT_IMAD / _HYBRID / _FP64
+
+
+def _tuning_dict(t):
+    return {"msm_product": MSM_PRODUCTS[t.msm_product], "ntt_cols_per_cta": t.ntt_cols_per_cta,
+            "ntt_threads": t.ntt_threads, "msm_ms": [round(x, 4) for x in t.msm_ms],
+            "ntt_ms": [round(x, 4) for x in t.ntt_ms]}
+
+
 _P = ctypes.c_void_p
 _SZ = ctypes.c_size_t
 class _Request(ctypes.Structure):
@@ -87,6 +102,9 @@ _SIGS = {
     "zg_encode_batch": (ctypes.c_int, [_P, _SZ, ctypes.POINTER(ctypes.c_void_p), ctypes.POINTER(_SZ), ctypes.c_int,
                                        ctypes.POINTER(_P)]),
     "zg_ctx_create": (ctypes.c_int, [ctypes.POINTER(_Config), ctypes.POINTER(_P)]),
+    "zg_ctx_autotune": (ctypes.c_int, [_P, ctypes.POINTER(_Tuning)]),
+    "zg_ctx_get_tuning": (ctypes.c_int, [_P, ctypes.POINTER(_Tuning)]),
+    "zg_ctx_set_tuning": (ctypes.c_int, [_P, ctypes.POINTER(_Tuning)]),
     "zg_ctx_destroy": (None, [_P]),
     "zg_ctx_warmup": (ctypes.c_int, [_P]),
     "zg_encode": (ctypes.c_int, [_P, ctypes.c_char_p, _SZ, ctypes.c_int, ctypes.POINTER(_P)]),
@@ -285,6 +303,24 @@ class ZgEncoderParams:
         buf = ctypes.create_string_buffer(n)
         _check(lib().zg_ctx_param_points(self._h, coset, line, first, count, buf, n))
         return buf.raw
+
+    def autotune(self):
+        """Time the kernels' free choices on a synthetic blob and keep the
+        fastest (zg_ctx_autotune); returns the choice and the times."""
+        t = _Tuning()
+        _check(lib().zg_ctx_autotune(self.handle, ctypes.byref(t)))
+        return _tuning_dict(t)
+
+    def tuning(self):
+        t = _Tuning()
+        _check(lib().zg_ctx_get_tuning(self.handle, ctypes.byref(t)))
+        return _tuning_dict(t)
+
+    def set_tuning(self, msm_product="hybrid", ntt_cols_per_cta=2, ntt_threads=256):
+        t = _Tuning()
+        t.msm_product = MSM_PRODUCTS.index(msm_product)
+        t.ntt_cols_per_cta, t.ntt_threads = ntt_cols_per_cta, ntt_threads
+        _check(lib().zg_ctx_set_tuning(self.handle, ctypes.byref(t)))
 
     def set_profiling(self, enable=True):
         _check(lib().zg_ctx_set_profiling(self._h, 1 if enable else 0))

@@ -10,37 +10,76 @@
 
 namespace zg {
 
-// Field products of the curve formulas go through one out-of-line device
-// function: the formulas then compile to a few hundred instructions that stay
+// Field products of the curve formulas go through out-of-line device
+// functions: the formulas then compile to a few hundred instructions that stay
 // in the instruction cache, instead of ten inlined ~300-instruction products
-// per point addition (host builds inline it).
-// Independent products are issued in pairs. On the device the pair runs on two
-// pipes at once: the first product on the integer multiply-add pipe (Fq::mul,
-// whose carry-chain IMADs saturate that pipe in the MSM bucket loop) and the
-// second on the FP64 pipe (f52::mont_mul, same value). Measured on the
-// 64 x 1024 encode, the MSM phase takes 4.5 % less time than with both
-// products on the integer pipe.
+// per point addition (host builds inline them). Independent products are
+// issued in pairs. Three interchangeable product kinds (same values):
+//   MulImad   both products of a pair on the integer multiply-add pipe
+//             (Fq::mul2, the two CIOS carry chains interleaved);
+//   MulHybrid the first on the integer pipe (Fq::mul), the second on the FP64
+//             pipe (f52::mont_mul): the MSM bucket loop saturates the integer
+//             pipe with carry-chain IMADs, so this pair keeps both pipes busy;
+//   MulF64    both on the FP64 pipe.
+// The curve formulas are templates over the kind; one kernel uses one kind
+// only (two product functions in one hot loop overflow the instruction
+// cache). MulHybrid is the default; the MSM kernel comes in all three and the
+// context's tuning picks one (on the B200 the hybrid pair is fastest).
 struct FqPair {
   Fq a, b;
 };
 #if defined(__CUDA_ARCH__) && !defined(ZG_INLINE_FMUL)
 static __device__ __noinline__ Fq fq_mul_ool(const Fq a, const Fq b) { return Fq::mul(a, b); }
-static __device__ __noinline__ FqPair fq_mul2_ool(const Fq a, const Fq b, const Fq c, const Fq d) {
+static __device__ __noinline__ FqPair fq_mul2_imad_ool(const Fq a, const Fq b, const Fq c, const Fq d) {
+  FqPair r;
+  Fq::mul2(a, b, c, d, r.a, r.b);
+  return r;
+}
+static __device__ __noinline__ FqPair fq_mul2_hybrid_ool(const Fq a, const Fq b, const Fq c, const Fq d) {
   FqPair r;
   r.a = Fq::mul(a, b);
   r.b = f52::mont_mul(c, d);
   return r;
 }
-#define ZG_FMUL(a, b) fq_mul_ool((a), (b))
-#define ZG_FMUL2(a, b, c, d) fq_mul2_ool((a), (b), (c), (d))
-#else
-#define ZG_FMUL(a, b) Fq::mul((a), (b))
-ZG_HD FqPair zg_fmul2_inline(const Fq& a, const Fq& b, const Fq& c, const Fq& d) {
+static __device__ __noinline__ Fq fq_mul_f64_ool(const Fq a, const Fq b) { return f52::mont_mul(a, b); }
+static __device__ __noinline__ FqPair fq_mul2_f64_ool(const Fq a, const Fq b, const Fq c, const Fq d) {
   FqPair r;
-  Fq::mul2(a, b, c, d, r.a, r.b);
+  r.a = f52::mont_mul(a, b);
+  r.b = f52::mont_mul(c, d);
   return r;
 }
-#define ZG_FMUL2(a, b, c, d) zg_fmul2_inline((a), (b), (c), (d))
+struct MulImad {
+  static __device__ __forceinline__ Fq mul(const Fq& a, const Fq& b) { return fq_mul_ool(a, b); }
+  static __device__ __forceinline__ FqPair mul2(const Fq& a, const Fq& b, const Fq& c, const Fq& d) {
+    return fq_mul2_imad_ool(a, b, c, d);
+  }
+};
+struct MulHybrid {
+  static __device__ __forceinline__ Fq mul(const Fq& a, const Fq& b) { return fq_mul_ool(a, b); }
+  static __device__ __forceinline__ FqPair mul2(const Fq& a, const Fq& b, const Fq& c, const Fq& d) {
+    return fq_mul2_hybrid_ool(a, b, c, d);
+  }
+};
+struct MulF64 {
+  static __device__ __forceinline__ Fq mul(const Fq& a, const Fq& b) { return fq_mul_f64_ool(a, b); }
+  static __device__ __forceinline__ FqPair mul2(const Fq& a, const Fq& b, const Fq& c, const Fq& d) {
+    return fq_mul2_f64_ool(a, b, c, d);
+  }
+};
+#else
+// host builds: the same values through Fq::mul; three distinct types so that
+// kernel templates keep one instance per kind in both compilation passes
+struct MulHost {
+  static ZG_HD Fq mul(const Fq& a, const Fq& b) { return Fq::mul(a, b); }
+  static ZG_HD FqPair mul2(const Fq& a, const Fq& b, const Fq& c, const Fq& d) {
+    FqPair r;
+    Fq::mul2(a, b, c, d, r.a, r.b);
+    return r;
+  }
+};
+struct MulImad : MulHost {};
+struct MulHybrid : MulHost {};
+struct MulF64 : MulHost {};
 #endif
 
 struct G1Aff {
@@ -63,14 +102,15 @@ struct XYZZ {
   }
 
   // 2 * (x, y) for an affine point (mdbl-2008-s)
+  template <class M = MulHybrid>
   ZG_HD static XYZZ dbl_affine(const Fq& x, const Fq& y) {
     Fq U = y + y;
-    FqPair vx = ZG_FMUL2(U, U, x, x);        // V = U^2, xx = x^2
-    Fq M = vx.b + vx.b + vx.b;
-    FqPair ws = ZG_FMUL2(U, vx.a, x, vx.a);  // W = U V, S = x V
+    FqPair vx = M::mul2(U, U, x, x);        // V = U^2, xx = x^2
+    Fq Mv = vx.b + vx.b + vx.b;
+    FqPair ws = M::mul2(U, vx.a, x, vx.a);  // W = U V, S = x V
     XYZZ r;
-    r.X = ZG_FMUL(M, M) - (ws.b + ws.b);
-    FqPair y3 = ZG_FMUL2(M, ws.b - r.X, ws.a, y);
+    r.X = M::mul(Mv, Mv) - (ws.b + ws.b);
+    FqPair y3 = M::mul2(Mv, ws.b - r.X, ws.a, y);
     r.Y = y3.a - y3.b;
     r.ZZ = vx.a;
     r.ZZZ = ws.a;
@@ -78,41 +118,43 @@ struct XYZZ {
   }
 
   // dbl-2008-s-1 (a = 0)
+  template <class M = MulHybrid>
   ZG_HD XYZZ dbl() const {
     if (is_inf()) return *this;
     Fq U = Y + Y;
-    FqPair vx = ZG_FMUL2(U, U, X, X);        // V, XX
-    Fq M = vx.b + vx.b + vx.b;
-    FqPair ws = ZG_FMUL2(U, vx.a, X, vx.a);  // W, S
-    FqPair mz = ZG_FMUL2(M, M, vx.a, ZZ);    // M^2, V ZZ
+    FqPair vx = M::mul2(U, U, X, X);        // V, XX
+    Fq Mv = vx.b + vx.b + vx.b;
+    FqPair ws = M::mul2(U, vx.a, X, vx.a);  // W, S
+    FqPair mz = M::mul2(Mv, Mv, vx.a, ZZ);  // M^2, V ZZ
     XYZZ r;
     r.X = mz.a - (ws.b + ws.b);
-    FqPair y3 = ZG_FMUL2(M, ws.b - r.X, ws.a, Y);
+    FqPair y3 = M::mul2(Mv, ws.b - r.X, ws.a, Y);
     r.Y = y3.a - y3.b;
     r.ZZ = mz.b;
-    r.ZZZ = ZG_FMUL(ws.a, ZZZ);
+    r.ZZZ = M::mul(ws.a, ZZZ);
     return r;
   }
 
   // this + (x2, y2) (madd-2008-s)
+  template <class M = MulHybrid>
   ZG_HD void add_affine(const Fq& x2, const Fq& y2) {
     if (is_inf()) {
       X = x2; Y = y2; ZZ = Fq::one(); ZZZ = Fq::one();
       return;
     }
-    FqPair us = ZG_FMUL2(x2, ZZ, y2, ZZZ);   // U2, S2
+    FqPair us = M::mul2(x2, ZZ, y2, ZZZ);   // U2, S2
     Fq P = us.a - X;
     Fq R = us.b - Y;
     if (P.is_zero()) {
-      if (R.is_zero()) *this = dbl_affine(x2, y2);
+      if (R.is_zero()) *this = dbl_affine<M>(x2, y2);
       else *this = inf();
       return;
     }
-    FqPair pr = ZG_FMUL2(P, P, R, R);        // PP, R^2
-    FqPair pq = ZG_FMUL2(P, pr.a, X, pr.a);  // PPP, Q
-    FqPair zz = ZG_FMUL2(ZZ, pr.a, ZZZ, pq.a);
+    FqPair pr = M::mul2(P, P, R, R);        // PP, R^2
+    FqPair pq = M::mul2(P, pr.a, X, pr.a);  // PPP, Q
+    FqPair zz = M::mul2(ZZ, pr.a, ZZZ, pq.a);
     Fq X3 = pr.b - pq.a - (pq.b + pq.b);
-    FqPair y3 = ZG_FMUL2(R, pq.b - X3, Y, pq.a);
+    FqPair y3 = M::mul2(R, pq.b - X3, Y, pq.a);
     X = X3;
     Y = y3.a - y3.b;
     ZZ = zz.a;
@@ -120,24 +162,25 @@ struct XYZZ {
   }
 
   // this + o (add-2008-s)
+  template <class M = MulHybrid>
   ZG_HD void add(const XYZZ& o) {
     if (o.is_inf()) return;
     if (is_inf()) { *this = o; return; }
-    FqPair u = ZG_FMUL2(X, o.ZZ, o.X, ZZ);     // U1, U2
-    FqPair sv = ZG_FMUL2(Y, o.ZZZ, o.Y, ZZZ);  // S1, S2
+    FqPair u = M::mul2(X, o.ZZ, o.X, ZZ);     // U1, U2
+    FqPair sv = M::mul2(Y, o.ZZZ, o.Y, ZZZ);  // S1, S2
     Fq P = u.b - u.a;
     Fq R = sv.b - sv.a;
     if (P.is_zero()) {
-      if (R.is_zero()) *this = dbl();
+      if (R.is_zero()) *this = dbl<M>();
       else *this = inf();
       return;
     }
-    FqPair pr = ZG_FMUL2(P, P, R, R);          // PP, R^2
-    FqPair pq = ZG_FMUL2(P, pr.a, u.a, pr.a);  // PPP, Q
-    FqPair zt = ZG_FMUL2(ZZ, o.ZZ, ZZZ, o.ZZZ);
+    FqPair pr = M::mul2(P, P, R, R);          // PP, R^2
+    FqPair pq = M::mul2(P, pr.a, u.a, pr.a);  // PPP, Q
+    FqPair zt = M::mul2(ZZ, o.ZZ, ZZZ, o.ZZZ);
     Fq X3 = pr.b - pq.a - (pq.b + pq.b);
-    FqPair y3 = ZG_FMUL2(R, pq.b - X3, sv.a, pq.a);
-    FqPair zz = ZG_FMUL2(zt.a, pr.a, zt.b, pq.a);
+    FqPair y3 = M::mul2(R, pq.b - X3, sv.a, pq.a);
+    FqPair zz = M::mul2(zt.a, pr.a, zt.b, pq.a);
     X = X3;
     Y = y3.a - y3.b;
     ZZ = zz.a;

@@ -15,6 +15,7 @@
 #include <mutex>
 #include <thread>
 #include <deque>
+#include <functional>
 #include <string>
 #include <vector>
 
@@ -221,7 +222,13 @@ struct zg_ctx {
   XYZZ* fb_T = nullptr;
   XYZZ* fb_S = nullptr;
   XYZZ* fb_gbuf = nullptr;  // per persistent CTA task partial sums
-  unsigned fb_ctas = 0;
+  unsigned fb_ctas[3] = {0, 0, 0};  // resident CTAs of k_fb_accum per product kind
+  // free choices of the kernels (zg_ctx_autotune / zg_ctx_set_tuning); the
+  // defaults are the fastest on the B200. tuning_gen counts changes, so the
+  // request pipeline re-captures its CUDA graphs.
+  uint32_t msm_product = ZG_MSM_PRODUCT_HYBRID;
+  uint32_t ntt_cpb = 2, ntt_threads = 256;
+  uint64_t tuning_gen = 0;
   uint8_t* raw = nullptr;
   uint8_t* enc = nullptr;
   Fr* T1 = nullptr;
@@ -313,11 +320,17 @@ int alloc_blob_buffers(zg_ctx* c) {
     ZG_CK(cudaMalloc(&c->fb_ents, 3 * R * FB_WINDOWS * c->C * sizeof(uint16_t)));
     ZG_CK(cudaMalloc(&c->fb_T, 3 * R * (size_t)c->L * FB_ACC_THREADS * sizeof(XYZZ)));
     ZG_CK(cudaMalloc(&c->fb_S, 3 * R * (size_t)c->L * FB_ACC_THREADS * sizeof(XYZZ)));
-    int sms = 0, per_sm = 0;
+    int sms = 0, per_sm[3] = {0, 0, 0};
     ZG_CK(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, c->device));
-    ZG_CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_fb_accum, FB_ACC_THREADS, 0));
-    c->fb_ctas = (unsigned)std::max(1, sms * std::max(1, per_sm));
-    ZG_CK(cudaMalloc(&c->fb_gbuf, (size_t)c->fb_ctas * FB_MAX_TASKS * sizeof(XYZZ)));
+    ZG_CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm[0], k_fb_accum<MulImad>, FB_ACC_THREADS, 0));
+    ZG_CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm[1], k_fb_accum<MulHybrid>, FB_ACC_THREADS, 0));
+    ZG_CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm[2], k_fb_accum<MulF64>, FB_ACC_THREADS, 0));
+    unsigned most = 1;
+    for (int k = 0; k < 3; ++k) {
+      c->fb_ctas[k] = (unsigned)std::max(1, sms * std::max(1, per_sm[k]));
+      most = std::max(most, c->fb_ctas[k]);
+    }
+    ZG_CK(cudaMalloc(&c->fb_gbuf, (size_t)most * FB_MAX_TASKS * sizeof(XYZZ)));
   }
   ZG_CK(cudaMalloc(&c->raw, c->max_blob + 16));
   ZG_CK(cudaMalloc(&c->enc, 3 * N * 32));
@@ -491,6 +504,54 @@ BlobBufs ctx_bufs(zg_ctx* c) {
 // trees, serialisation, slices.
 uint64_t launches_per_encode(const zg_ctx* c) { return 3 + (uint64_t)c->tree_depth + 1 + 1 + (c->fb ? 3 : 2) + 1 + 1 + 1; }
 
+// the blob MSM's work items: (coset, chunk, line) over the context's tables
+FbAccArgs blob_fb_args(const zg_ctx* c) {
+  FbAccArgs fa;
+  fa.tab = c->tab;
+  fa.offs = c->fb_offs;
+  fa.ents = c->fb_ents;
+  fa.outT = c->fb_T;
+  fa.outS = c->fb_S;
+  fa.lr = c->lr;
+  fa.lc = c->lc;
+  fa.lines = c->L;
+  fa.tabN = c->N;
+  return fa;
+}
+
+// seeded pseudo-random payload bytes (the autotuner's synthetic blob)
+__global__ void k_fill_payload(uint8_t* p, uint64_t n, uint64_t seed) {
+  for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (uint64_t)gridDim.x * blockDim.x) {
+    uint64_t z = (i >> 3) * 0x9e3779b97f4a7c15ull + seed;
+    z = (z ^ (z >> 30)) * 0xbf58476d1ce4e5b9ull;
+    z = (z ^ (z >> 27)) * 0x94d049bb133111ebull;
+    z ^= z >> 31;
+    p[i] = (uint8_t)(z >> (8 * (i & 7)));
+  }
+}
+
+// k_fb_accum over `units` work items with product kind `kind`
+void launch_fb_accum(const zg_ctx* c, uint32_t kind, const FbAccArgs& fa, uint32_t units, cudaStream_t s) {
+  const unsigned grid = std::min<unsigned>(c->fb_ctas[kind], units);
+  if (kind == ZG_MSM_PRODUCT_IMAD) k_fb_accum<MulImad><<<grid, FB_ACC_THREADS, 0, s>>>(fa, c->fb_gbuf, units);
+  else if (kind == ZG_MSM_PRODUCT_FP64) k_fb_accum<MulF64><<<grid, FB_ACC_THREADS, 0, s>>>(fa, c->fb_gbuf, units);
+  else k_fb_accum<MulHybrid><<<grid, FB_ACC_THREADS, 0, s>>>(fa, c->fb_gbuf, units);
+}
+
+// the three RS-extension passes with a given column tile and block size
+void launch_rs(const zg_ctx* c, const uint8_t* raw, size_t len, const uint64_t* d_len, uint8_t* enc, uint32_t cpb,
+               uint32_t threads, cudaStream_t s) {
+  const int lr = c->lr, lc = c->lc;
+  const size_t R = c->R, C = c->C;
+  k_rows_from_raw<<<(unsigned)R, threads, C * sizeof(Fr) + 31 * C, s>>>(raw, len, d_len, c->max_raw, lr, lc, enc,
+                                                                        c->T1, c->tw.twi_c, c->tw.wni_lo,
+                                                                        c->tw.wni_hi);
+  k_cols<<<nblk(C, cpb), threads, 2 * R * sizeof(Fr), s>>>(c->T1, c->Bc, lr, lc, c->tw.twi_r, c->tw.twf_r,
+                                                            c->tw.gs_lo, c->tw.gs_hi, c->tw.wn_lo, c->tw.wn_hi,
+                                                            (int)cpb);
+  k_rows_ntt<<<dim3((unsigned)R, 2), threads, C * sizeof(Fr), s>>>(c->Bc, enc, lr, lc, c->tw.twf_c);
+}
+
 // The per-blob pipeline on the device, launches only. The payload is `len`
 // bytes at b.raw, or *b.d_len bytes when `by_device_len` (graph capture).
 int encode_launches(zg_ctx* c, const BlobBufs& b, size_t len, bool by_device_len, cudaStream_t s, bool marks) {
@@ -501,13 +562,7 @@ int encode_launches(zg_ctx* c, const BlobBufs& b, size_t len, bool by_device_len
   };
   mark(0);
   // RS extension: rows iNTT, column passes, rows NTT
-  k_rows_from_raw<<<(unsigned)R, 256, C * sizeof(Fr) + 31 * C, s>>>(
-      b.raw, len, by_device_len ? b.d_len : nullptr, c->max_raw, lr, lc, b.enc, c->T1, c->tw.twi_c, c->tw.wni_lo,
-      c->tw.wni_hi);
-  k_cols<<<nblk(C, COLS_PER_BLOCK), 256, 2 * R * sizeof(Fr), s>>>(c->T1, c->Bc, lr, lc, c->tw.twi_r, c->tw.twf_r,
-                                                                   c->tw.gs_lo, c->tw.gs_hi, c->tw.wn_lo,
-                                                                   c->tw.wn_hi);
-  k_rows_ntt<<<dim3((unsigned)R, 2), 256, C * sizeof(Fr), s>>>(c->Bc, b.enc, lr, lc, c->tw.twf_c);
+  launch_rs(c, b.raw, len, by_device_len ? b.d_len : nullptr, b.enc, c->ntt_cpb, c->ntt_threads, s);
   int rc = check_launch();
   if (rc) return rc;
   mark(1);
@@ -519,18 +574,8 @@ int encode_launches(zg_ctx* c, const BlobBufs& b, size_t len, bool by_device_len
   if (c->fb) {
     k_fb_sort<<<dim3((unsigned)R, 3), 256, fb_sort_smem_bytes(lc), s>>>(b.enc, c->fb_offs, c->fb_ents, lr, lc, 1,
                                                                          N);
-    FbAccArgs fa;
-    fa.tab = c->tab;
-    fa.offs = c->fb_offs;
-    fa.ents = c->fb_ents;
-    fa.outT = c->fb_T;
-    fa.outS = c->fb_S;
-    fa.lr = lr;
-    fa.lc = lc;
-    fa.lines = c->L;
-    fa.tabN = N;
     const uint32_t units = (uint32_t)(3 * R * c->L);
-    k_fb_accum<<<std::min<unsigned>(c->fb_ctas, units), FB_ACC_THREADS, 0, s>>>(fa, c->fb_gbuf, units);
+    launch_fb_accum(c, c->msm_product, blob_fb_args(c), units, s);
     mark(3);
     k_fb_combine<<<nblk(units, 64), 64, 0, s>>>(c->fb_T, c->fb_S, c->part, lr, c->L, units);
   } else {
@@ -737,6 +782,7 @@ struct Slot {
   uint8_t* h_small = nullptr;  // pinned: [0,8) length, [8,200) coset commitments, [200,296) roots, [296,328) file root
   cudaEvent_t ev_in = nullptr, ev_comp = nullptr, ev_out = nullptr;
   cudaGraphExec_t graph = nullptr;
+  uint64_t gen = 0;        // the context's tuning_gen when the graph was captured
   Request* req = nullptr;  // reserved for / in flight in this slot
 };
 
@@ -765,8 +811,14 @@ void complete(Engine* e, Request* q, int status, const std::string& err) {
 }
 
 int slot_graph(Engine* e, Slot& sl) {
-  if (sl.graph || !e->use_graph) return 0;
   zg_ctx* c = e->c;
+  // a tuning change since the capture: the old graph's last launch preceded
+  // the change, which synchronised the context's stream
+  if (sl.graph && sl.gen != c->tuning_gen) {
+    cudaGraphExecDestroy(sl.graph);
+    sl.graph = nullptr;
+  }
+  if (sl.graph || !e->use_graph) return 0;
   cudaStream_t cs = nullptr;
   ZG_CK(cudaStreamCreateWithFlags(&cs, cudaStreamNonBlocking));
   cudaGraph_t g = nullptr;
@@ -777,6 +829,7 @@ int slot_graph(Engine* e, Slot& sl) {
     err = cudaStreamEndCapture(cs, &g);
   }
   if (err == cudaSuccess && rc == 0) err = cudaGraphInstantiate(&sl.graph, g, 0);
+  sl.gen = c->tuning_gen;
   if (g) cudaGraphDestroy(g);
   cudaStreamDestroy(cs);
   if (err != cudaSuccess || rc) {  // launch the kernels one by one instead
@@ -1329,6 +1382,102 @@ int zg_ctx_param_points(zg_ctx* c, int coset, int line, size_t first, size_t cou
   return ZG_OK;
 }
 
+int zg_ctx_get_tuning(zg_ctx* c, zg_tuning* out) {
+  if (!c || !out) return fail(ZG_ERR_INVALID_ARG, "null argument");
+  std::lock_guard<std::mutex> g(c->mu);
+  memset(out, 0, sizeof(*out));
+  out->msm_product = c->msm_product;
+  out->ntt_cols_per_cta = c->ntt_cpb;
+  out->ntt_threads = c->ntt_threads;
+  return ZG_OK;
+}
+
+namespace {
+bool tuning_valid(const zg_tuning* t) {
+  const uint32_t cpb = t->ntt_cols_per_cta, th = t->ntt_threads;
+  return t->msm_product <= ZG_MSM_PRODUCT_FP64 && (cpb == 1 || cpb == 2 || cpb == 4) &&
+         (th == 128 || th == 256 || th == 512);
+}
+}  // namespace
+
+int zg_ctx_set_tuning(zg_ctx* c, const zg_tuning* t) {
+  if (!c || !t) return fail(ZG_ERR_INVALID_ARG, "null argument");
+  if (!tuning_valid(t))
+    return fail(ZG_ERR_INVALID_ARG, "tuning: msm_product 0..2, ntt_cols_per_cta 1/2/4, ntt_threads 128/256/512");
+  std::lock_guard<std::mutex> g(c->mu);
+  ZG_CK(cudaSetDevice(c->device));
+  ZG_CK(cudaEventSynchronize(c->done));  // no launch with the old choices is in flight
+  c->msm_product = t->msm_product;
+  c->ntt_cpb = t->ntt_cols_per_cta;
+  c->ntt_threads = t->ntt_threads;
+  ++c->tuning_gen;
+  return ZG_OK;
+}
+
+int zg_ctx_autotune(zg_ctx* c, zg_tuning* out) {
+  if (!c) return fail(ZG_ERR_INVALID_ARG, "null context");
+  std::lock_guard<std::mutex> g(c->mu);
+  ZG_CK(cudaSetDevice(c->device));
+  cudaStream_t s = c->stream;
+  ZG_CK(cudaStreamWaitEvent(s, c->done, 0));
+  zg_tuning t;
+  memset(&t, 0, sizeof(t));
+  // a full-size synthetic blob on the context's own buffers; its encode also
+  // leaves the MSM's sorted digits in place for the kernel samples below
+  const size_t len = c->max_raw;
+  k_fill_payload<<<(unsigned)std::min<size_t>(nblk(len, 256), 4096), 256, 0, s>>>(c->raw, len, 0x5eedull);
+  int rc = encode_launches(c, ctx_bufs(c), len, false, s, false);
+  if (rc) return rc;
+  cudaEvent_t e0 = nullptr, e1 = nullptr;
+  ZG_CK(cudaEventCreate(&e0));
+  ZG_CK(cudaEventCreate(&e1));
+  auto timed = [&](const std::function<void()>& fn) -> float {
+    fn();  // warm-up
+    cudaEventRecord(e0, s);
+    fn();
+    cudaEventRecord(e1, s);
+    float ms = -1.f;
+    if (cudaEventSynchronize(e1) == cudaSuccess) cudaEventElapsedTime(&ms, e0, e1);
+    return ms;
+  };
+  uint32_t best_msm = c->msm_product;
+  if (c->fb) {
+    // a sample of every line's work items: the first 4 per resident CTA
+    const uint32_t all = (uint32_t)(3 * c->R * c->L);
+    const uint32_t sample = std::min<uint32_t>(all, 4 * std::max(c->fb_ctas[0], std::max(c->fb_ctas[1], c->fb_ctas[2])));
+    const FbAccArgs fa = blob_fb_args(c);
+    float best = 0;
+    for (uint32_t k = 0; k < 3; ++k) {
+      t.msm_ms[k] = timed([&] { launch_fb_accum(c, k, fa, sample, s); });
+      if (t.msm_ms[k] > 0 && (best == 0 || t.msm_ms[k] < best)) { best = t.msm_ms[k]; best_msm = k; }
+    }
+  }
+  const uint32_t cpbs[3] = {1, 2, 4}, ths[3] = {128, 256, 512};
+  uint32_t best_cpb = c->ntt_cpb, best_th = c->ntt_threads;
+  float best = 0;
+  for (int i = 0; i < 3; ++i)
+    for (int j = 0; j < 3; ++j) {
+      float ms = timed([&] { launch_rs(c, c->raw, len, nullptr, c->enc, cpbs[i], ths[j], s); });
+      t.ntt_ms[3 * i + j] = ms;
+      if (ms > 0 && (best == 0 || ms < best)) { best = ms; best_cpb = cpbs[i]; best_th = ths[j]; }
+    }
+  rc = check_launch();
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  if (rc) return rc;
+  ZG_CK(cudaEventRecord(c->done, s));
+  ZG_CK(cudaStreamSynchronize(s));
+  c->msm_product = best_msm;
+  c->ntt_cpb = best_cpb;
+  c->ntt_threads = best_th;
+  ++c->tuning_gen;
+  t.msm_product = best_msm;
+  t.ntt_cols_per_cta = best_cpb;
+  t.ntt_threads = best_th;
+  if (out) *out = t;
+  return ZG_OK;
+}
+
 int zg_ctx_set_profiling(zg_ctx* c, int enable) {
   if (!c) return fail(ZG_ERR_INVALID_ARG, "null context");
   std::lock_guard<std::mutex> g(c->mu);
@@ -1548,7 +1697,7 @@ int zg_ctx_msm(zg_ctx* c, uint32_t coset, uint32_t line, const void* d_scalars, 
   fa.lc = c->lc;
   fa.lines = 1;
   fa.tabN = c->N;
-  k_fb_accum<<<std::min<unsigned>(c->fb_ctas, nch), FB_ACC_THREADS, 0, s>>>(fa, c->fb_gbuf, nch);
+  launch_fb_accum(c, c->msm_product, fa, nch, s);
   k_fb_combine<<<nblk(nch, 64), 64, 0, s>>>(c->fb_T, c->fb_S, c->part, lrn, 1, nch);
   k_sum_points<<<1, 256, 0, s>>>(c->part, nch, c->nodes);
   k_serialize_nodes<<<1, 128, 0, s>>>(c->nodes, (uint8_t*)d_out, 1);

@@ -73,7 +73,7 @@ __device__ __forceinline__ Fr pow_split(const Fr* lo, const Fr* hi, uint32_t e, 
 // raw_blob.rs:33-40).
 // The payload length is `len`, or *d_len when d_len is set (graph launches,
 // whose parameters are fixed at capture).
-__global__ void __launch_bounds__(256) k_rows_from_raw(const uint8_t* __restrict__ raw, uint64_t len,
+__global__ void __launch_bounds__(512) k_rows_from_raw(const uint8_t* __restrict__ raw, uint64_t len,
                                                        const uint64_t* __restrict__ d_len, uint64_t max_raw, int lr,
                                                        int lc, uint8_t* __restrict__ enc0, Fr* __restrict__ T1,
                                                        const Fr* __restrict__ twi_c, const Fr* __restrict__ wni_lo,
@@ -122,18 +122,19 @@ __global__ void __launch_bounds__(256) k_rows_from_raw(const uint8_t* __restrict
 // Pass 2: per column s, iNTT over rows (size R), then per extension coset
 // c in {1, 2}: scale coefficient m = s + C q by g_c^m / N, forward NTT over q,
 // multiply by w_N^{s r}; store Bc[c-1][r][s].
-constexpr int COLS_PER_BLOCK = 2;
-__global__ void __launch_bounds__(256) k_cols(const Fr* __restrict__ T1, Fr* __restrict__ Bc, int lr, int lc,
+// One CTA handles `cpb` consecutive columns one after the other (a tuning
+// knob: fewer, longer CTAs against more, shorter ones).
+__global__ void __launch_bounds__(512) k_cols(const Fr* __restrict__ T1, Fr* __restrict__ Bc, int lr, int lc,
                        const Fr* __restrict__ twi_r, const Fr* __restrict__ twf_r,
                        const Fr* __restrict__ gs_lo, const Fr* __restrict__ gs_hi,
-                       const Fr* __restrict__ wn_lo, const Fr* __restrict__ wn_hi) {
+                       const Fr* __restrict__ wn_lo, const Fr* __restrict__ wn_hi, int cpb) {
   extern __shared__ __align__(16) uint8_t smem[];
   const int R = 1 << lr, C = 1 << lc;
   Fr* coef = reinterpret_cast<Fr*>(smem);
   Fr* work = coef + (size_t)R;
   const uint32_t nmask = (1u << (lr + lc)) - 1;
-  for (int cc = 0; cc < COLS_PER_BLOCK; ++cc) {
-    const uint32_t s = blockIdx.x * COLS_PER_BLOCK + cc;
+  for (int cc = 0; cc < cpb; ++cc) {
+    const uint32_t s = blockIdx.x * cpb + cc;
     if (s >= (uint32_t)C) break;
     for (int r = threadIdx.x; r < R; r += blockDim.x)
       coef[brev_bits(r, lr)] = load_fr(T1 + (size_t)r * C + s);
@@ -156,7 +157,7 @@ __global__ void __launch_bounds__(256) k_cols(const Fr* __restrict__ T1, Fr* __r
 
 // Pass 3: per coset c in {1,2} and row r, forward NTT over s (size C):
 // enc[c][r][j] = canonical( sum_s v_C^{s j} Bc[c-1][r][s] ).
-__global__ void __launch_bounds__(256) k_rows_ntt(const Fr* __restrict__ Bc, uint8_t* __restrict__ enc, int lr, int lc,
+__global__ void __launch_bounds__(512) k_rows_ntt(const Fr* __restrict__ Bc, uint8_t* __restrict__ enc, int lr, int lc,
                            const Fr* __restrict__ twf_c) {
   extern __shared__ __align__(16) uint8_t smem[];
   const int R = 1 << lr, C = 1 << lc;
@@ -382,16 +383,16 @@ __global__ void __launch_bounds__(128) k_fb_tables(G1Aff* tab, uint64_t N, uint6
   Fq run = Fq::one();
   for (int w = 0; w < FB_WINDOWS - 1; ++w) {
     pre[w] = run;
-    run = ZG_FMUL(run, pts[w].ZZZ);
+    run = MulHybrid::mul(run, pts[w].ZZZ);
   }
   Fq inv = run.inverse();
   for (int w = FB_WINDOWS - 2; w >= 0; --w) {
-    Fq izzz = ZG_FMUL(inv, pre[w]);
-    inv = ZG_FMUL(inv, pts[w].ZZZ);
-    Fq izz = ZG_FMUL(ZG_FMUL(pts[w].ZZ, pts[w].ZZ), ZG_FMUL(izzz, izzz));
+    Fq izzz = MulHybrid::mul(inv, pre[w]);
+    inv = MulHybrid::mul(inv, pts[w].ZZZ);
+    Fq izz = MulHybrid::mul(MulHybrid::mul(pts[w].ZZ, pts[w].ZZ), MulHybrid::mul(izzz, izzz));
     G1Aff a;
-    a.x = ZG_FMUL(pts[w].X, izz);
-    a.y = ZG_FMUL(pts[w].Y, izzz);
+    a.x = MulHybrid::mul(pts[w].X, izz);
+    a.y = MulHybrid::mul(pts[w].Y, izzz);
     col[(uint64_t)(w + 1) * N] = a;
   }
 }
@@ -509,6 +510,9 @@ struct FbAccArgs {
 //     into running sums S_i = sum B_k, T_i = sum (k - 8i) B_k.
 constexpr int FB_TASK = 32;
 constexpr int FB_MAX_TASKS = FB_BUCKETS + FB_WINDOWS * 1024 / FB_TASK;  // chunk <= 1024 points
+// M is the product kind of the point additions (MulImad / MulHybrid / MulF64,
+// chosen by the context's tuning; identical results).
+template <class M>
 __global__ void __launch_bounds__(FB_ACC_THREADS, 4) k_fb_accum(FbAccArgs a, XYZZ* __restrict__ gpart_all,
                                                                 uint32_t units) {
   __shared__ uint32_t soffs[FB_BUCKETS + 1];
@@ -589,7 +593,7 @@ __global__ void __launch_bounds__(FB_ACC_THREADS, 4) k_fb_accum(FbAccArgs a, XYZ
         const uint32_t v = ents[e];
         G1Aff p = load_aff(tabl + (uint64_t)((v >> 10) & 31) * N + (v & 0x3ff));
         if (v & 0x8000) p.y = -p.y;
-        B.add_affine(p.x, p.y);
+        B.template add_affine<M>(p.x, p.y);
       }
       store_xyzz(gpart + t, B);
     }
@@ -597,8 +601,8 @@ __global__ void __launch_bounds__(FB_ACC_THREADS, 4) k_fb_accum(FbAccArgs a, XYZ
     const int k0 = threadIdx.x * FB_PER_THREAD;  // 0-based buckets k0 .. k0+7
     XYZZ S = XYZZ::inf(), T = XYZZ::inf();
     for (int k = k0 + FB_PER_THREAD - 1; k >= k0; --k) {
-      for (uint32_t t = tstart[k]; t < tstart[k + 1]; ++t) S.add(load_xyzz(gpart + t));
-      T.add(S);
+      for (uint32_t t = tstart[k]; t < tstart[k + 1]; ++t) S.template add<M>(load_xyzz(gpart + t));
+      T.template add<M>(S);
     }
     store_xyzz(a.outT + (size_t)u * FB_ACC_THREADS + threadIdx.x, T);
     store_xyzz(a.outS + (size_t)u * FB_ACC_THREADS + threadIdx.x, S);

@@ -94,6 +94,37 @@ int zg_encode_device(zg_ctx* ctx, const void* d_data, size_t len, void* stream, 
 int zg_ctx_param_points(zg_ctx* ctx, int coset, int line, size_t first, size_t count, uint8_t* host_out,
                         size_t cap);
 
+/* Tuning of the kernels' free choices (no reference counterpart: the
+ * reference's GPU plugin fixes its window width and launch shapes inside
+ * ag-cuda-ec, prove_gpu.rs:77). Every choice gives identical results.
+ *   msm_product      field products of the MSM point additions:
+ *                    ZG_MSM_PRODUCT_IMAD both products of each independent pair
+ *                    on the integer multiply-add pipe, ZG_MSM_PRODUCT_HYBRID one
+ *                    there and one on the FP64 pipe (default), ZG_MSM_PRODUCT_FP64
+ *                    both on the FP64 pipe;
+ *   ntt_cols_per_cta columns per CTA of the RS column pass: 1, 2 (default), 4;
+ *   ntt_threads      threads per CTA of the three RS passes: 128, 256 (default), 512.
+ * zg_ctx_autotune encodes a synthetic full-size blob on the context, times
+ * each MSM product kind on a sample of the blob's chunk MSMs and each NTT
+ * shape on the full RS extension, keeps the fastest and returns the choice
+ * with the times (ms; msm_ms[kind], ntt_ms[3 * i + j] for cols_per_cta
+ * {1, 2, 4}[i] and threads {128, 256, 512}[j]). It runs after the context's
+ * queued work and takes well under a second at production size; the request
+ * pipeline re-captures its CUDA graphs for the new choice. */
+#define ZG_MSM_PRODUCT_IMAD 0
+#define ZG_MSM_PRODUCT_HYBRID 1
+#define ZG_MSM_PRODUCT_FP64 2
+typedef struct zg_tuning {
+  uint32_t msm_product;
+  uint32_t ntt_cols_per_cta;
+  uint32_t ntt_threads;
+  float msm_ms[3];
+  float ntt_ms[9];
+} zg_tuning;
+int zg_ctx_autotune(zg_ctx* ctx, zg_tuning* out);
+int zg_ctx_get_tuning(zg_ctx* ctx, zg_tuning* out);
+int zg_ctx_set_tuning(zg_ctx* ctx, const zg_tuning* t);
+
 /* Measurement hooks (no reference counterpart; the reference logs tracing
  * spans, grpc/src/service.rs:68). With profiling on, every encode records CUDA
  * events between its phases; zg_ctx_phase_times returns the last encode's

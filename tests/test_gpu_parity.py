@@ -237,6 +237,49 @@ def test_encode_matches_oracle(gpu_pkg, oracle, log_row, log_col):
     params.close()
 
 
+@pytest.mark.parametrize("product,cpb,threads", [
+    ("imad", 1, 128), ("hybrid", 4, 512), ("fp64", 2, 256), ("imad", 2, 512), ("fp64", 4, 128),
+])
+def test_tuning_choices_match_oracle(gpu_pkg, oracle, product, cpb, threads):
+    """Every kernel choice the tuning can make (MSM product kind, RS column
+    tile and block size) gives the oracle's bytes, on the plain path and on
+    the request pipeline (whose CUDA graphs are re-captured on a change)."""
+    params = gpu_pkg.ZgEncoderParams.from_seed(5, 6, 17)
+    op = oracle.params(5, 6, 17)
+    payload = np.random.default_rng(cpb * threads).integers(0, 256, size=params.dims.max_raw_data_size - 3,
+                                                            dtype=np.uint8).tobytes()
+    exp = oracle.encode(op, payload)
+    # the pipeline first runs (and captures its graphs) with the default choice
+    first = gpu_pkg.EncoderService(params).process_batch([payload], True)[0]
+    assert first.storage_root == exp.file_root()
+    params.set_tuning(product, cpb, threads)
+    t = params.tuning()
+    assert (t["msm_product"], t["ntt_cols_per_cta"], t["ntt_threads"]) == (product, cpb, threads)
+    _check_against_oracle(gpu_pkg, oracle, params, op, payload)
+    again = gpu_pkg.EncoderService(params).process_batch([payload], True)[0]
+    assert again.encoded_slice == [exp.slice(i) for i in range(params.dims.rows_encoded)]
+    assert again.erasure_commitment == exp.commitment()
+    with pytest.raises(RuntimeError):
+        params.set_tuning(product, 3, threads)
+    params.close()
+
+
+def test_autotune_then_encode(gpu_pkg, oracle):
+    """zg_ctx_autotune times every candidate, keeps the fastest, and the
+    encodes after it still give the oracle's bytes."""
+    params = gpu_pkg.ZgEncoderParams.from_seed(6, 5, 23)
+    op = oracle.params(6, 5, 23)
+    t = params.autotune()
+    assert t["msm_product"] in gpu_pkg.MSM_PRODUCTS
+    assert all(x > 0 for x in t["msm_ms"]) and all(x > 0 for x in t["ntt_ms"])
+    k = gpu_pkg.MSM_PRODUCTS.index(t["msm_product"])
+    assert t["msm_ms"][k] == min(t["msm_ms"])
+    assert params.tuning()["msm_product"] == t["msm_product"]
+    payload = np.random.default_rng(5).integers(0, 256, size=4321, dtype=np.uint8).tobytes()
+    _check_against_oracle(gpu_pkg, oracle, params, op, payload)
+    params.close()
+
+
 @pytest.mark.parametrize("bits", [8, 11])
 def test_encode_msm_variants_match_oracle(gpu_pkg, oracle, bits):
     """Both MSM variants (8-bit windows with doublings; 11-bit fixed-base
