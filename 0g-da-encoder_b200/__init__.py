@@ -102,6 +102,9 @@ _SIGS = {
     "zg_encode_batch": (ctypes.c_int, [_P, _SZ, ctypes.POINTER(ctypes.c_void_p), ctypes.POINTER(_SZ), ctypes.c_int,
                                        ctypes.POINTER(_P)]),
     "zg_ctx_create": (ctypes.c_int, [ctypes.POINTER(_Config), ctypes.POINTER(_P)]),
+    "zg_verify_slices": (ctypes.c_int, [_P, ctypes.POINTER(ctypes.c_char_p), ctypes.POINTER(_SZ), _SZ,
+                                        ctypes.c_char_p, ctypes.c_char_p, ctypes.c_uint64,
+                                        ctypes.POINTER(ctypes.c_int32), ctypes.POINTER(ctypes.c_int64)]),
     "zg_ctx_autotune": (ctypes.c_int, [_P, ctypes.POINTER(_Tuning)]),
     "zg_ctx_get_tuning": (ctypes.c_int, [_P, ctypes.POINTER(_Tuning)]),
     "zg_ctx_set_tuning": (ctypes.c_int, [_P, ctypes.POINTER(_Tuning)]),
@@ -472,6 +475,26 @@ class LightEncodedSlice:
         _check(lib().zg_light_slice_into_slice(self.data, len(self.data), row, len(row), d.log_row, d.log_col,
                                                out, len(out), ctypes.byref(n)))
         return out.raw[:n.value]
+
+
+# EncodedSlice::verify verdicts (zg_verify_slices; the reference's VerifierError variants)
+V_OK = 0
+V_AMT_INCORRECT_PROOF = 14
+V_DESERIALIZE = 30
+
+
+def verify_slices(params: ZgEncoderParams, slices, commitment: bytes, storage_root: bytes, seed=0):
+    """EncodedSlice::verify (crates/encoder/src/encoder/slice.rs:73-95) for a
+    batch of serialized slices of one blob, on the GPU (zg_verify_slices).
+    Returns (codes, details): per slice the verdict code and its 4 detail
+    fields [AmtProofError, a, b, c]."""
+    n = len(slices)
+    ptrs = (ctypes.c_char_p * max(n, 1))(*slices)
+    lens = (ctypes.c_size_t * max(n, 1))(*[len(x) for x in slices])
+    codes = (ctypes.c_int32 * max(n, 1))()
+    det = (ctypes.c_int64 * max(4 * n, 1))()
+    _check(lib().zg_verify_slices(params.handle, ptrs, lens, n, commitment, storage_root, seed, codes, det))
+    return [codes[i] for i in range(n)], [[det[4 * i + k] for k in range(4)] for i in range(n)]
 
 
 class EncoderService:

@@ -16,12 +16,14 @@
 #include <thread>
 #include <deque>
 #include <functional>
+#include <random>
 #include <string>
 #include <vector>
 
 #include "../../include/zg_encoder.h"
 #include "zg_kernels.cuh"
 #include "zg_recover.cuh"
+#include "zg_verify.cuh"
 
 using namespace zg;
 
@@ -257,6 +259,15 @@ struct zg_ctx {
   uint16_t* rec_erased = nullptr;
   uint32_t* rec_err = nullptr;
   uint8_t* h_rec = nullptr;      // pinned staging (rows in, RawData out)
+  // G2 side of the params, for slice verification: g2 (the generator) and per
+  // coset high_g2 and the vanishing points (level d holds 2^(d+1) points at
+  // offset 2^(d+1) - 2). Read from the params files, or built from the seeded
+  // tau on the first verification.
+  bool g2_ready = false;
+  bool seeded = false;
+  uint64_t tau_seed = 0;
+  std::vector<G2Aff> vanish[3];
+  G2Aff high_g2[3];
   // measurement: optional per-phase events and a count of kernel launches
   bool profiling = false;
   cudaEvent_t ev[6] = {nullptr, nullptr, nullptr, nullptr, nullptr, nullptr};
@@ -415,6 +426,38 @@ int build_seeded_params(zg_ctx* c, uint64_t seed) {
 
 // reference mont files: amt-prove-coset{c}-mont-{hash}-{LR:02}-{LN:02}.bin
 // (crates/amt/src/utils.rs:20-45; format fast_serde_bn254.rs:20-88)
+// canonical little-endian field element (top `flag_bits` bits of the last
+// byte masked off) below the modulus
+template <class F>
+bool field_from_le(const uint8_t* b, F* out, uint8_t* flags = nullptr) {
+  F x;
+  for (int i = 0; i < 8; ++i)
+    x.v[i] = (uint32_t)b[4 * i] | (uint32_t)b[4 * i + 1] << 8 | (uint32_t)b[4 * i + 2] << 16 |
+             (uint32_t)b[4 * i + 3] << 24;
+  if (flags) {
+    *flags = (uint8_t)(x.v[7] >> 30);
+    x.v[7] &= 0x3fffffffu;
+  }
+  F d;
+  if (!F::sub_raw(d, x, F::modulus())) return false;  // x >= modulus
+  *out = F::from_canonical(x);
+  return true;
+}
+
+// ark-serialize uncompressed G2 (x.c0 | x.c1 | y.c0 | y.c1, flags in the top
+// bits of the last byte)
+bool g2_from_ark(const uint8_t* b, G2Aff* out) {
+  uint8_t fl = 0;
+  Fq t[4];
+  for (int k = 0; k < 4; ++k)
+    if (!field_from_le(b + 32 * k, &t[k], k == 3 ? &fl : nullptr)) return false;
+  if (fl == 3) return false;
+  out->inf = fl == 1;
+  out->x = Fq2{t[0], t[1]};
+  out->y = Fq2{t[2], t[3]};
+  return true;
+}
+
 int load_mont_params(zg_ctx* c, const char* dir) {
   const int ln = c->lr + c->lc;
   std::vector<uint8_t> hostline(c->N * 64);
@@ -439,20 +482,34 @@ int load_mont_params(zg_ctx* c, const char* dir) {
     if (!f) return fail(ZG_ERR_PARAMS, "cannot open " + found);
     uint8_t hdr[6];
     bool ok = fread(hdr, 1, 6, f) == 6 && memcmp(hdr, "bamt", 4) == 0 && hdr[4] == ln && hdr[5] == c->lr;
-    ok = ok && fseek(f, 256, SEEK_CUR) == 0;  // g2, high_g2 (uncompressed G2, 128 B each)
+    uint8_t g2b[256];
+    ok = ok && fread(g2b, 1, 256, f) == 256;  // g2, high_g2 (uncompressed G2, 128 B each)
+    ok = ok && g2_from_ark(g2b + 128, &c->high_g2[cs]);
     auto read_line = [&](G1Aff* dst) {
       if (fread(hostline.data(), 1, hostline.size(), f) != hostline.size()) return false;
       return cudaMemcpy(dst, hostline.data(), hostline.size(), cudaMemcpyHostToDevice) == cudaSuccess;
     };
     ok = ok && read_line(c->line_ptr(cs, c->lr));  // basis
     for (int d = 0; ok && d < c->lr; ++d) ok = read_line(c->line_ptr(cs, d));
-    size_t van = 0;
-    for (int d = 0; d < c->lr; ++d) van += (size_t)128 << (d + 1);
-    ok = ok && fseek(f, (long)van, SEEK_CUR) == 0;
+    // vanishing points: raw Montgomery x.c0 | x.c1 | y.c0 | y.c1 (fast_serde_bn254.rs:139-160)
+    c->vanish[cs].assign((size_t)2 * c->R - 2, G2Aff{});
+    for (size_t k = 0; ok && k < c->vanish[cs].size(); ++k) {
+      uint32_t w[32];
+      ok = fread(w, 1, 128, f) == 128;
+      G2Aff& g = c->vanish[cs][k];
+      for (int i = 0; i < 8; ++i) {
+        g.x.c0.v[i] = w[i];
+        g.x.c1.v[i] = w[8 + i];
+        g.y.c0.v[i] = w[16 + i];
+        g.y.c1.v[i] = w[24 + i];
+      }
+      g.inf = 0;
+    }
     ok = ok && read_line(c->line_ptr(cs, c->lr + 1));  // high_basis
     fclose(f);
     if (!ok) return fail(ZG_ERR_PARAMS, "malformed params file " + found);
   }
+  c->g2_ready = true;
   return 0;
 }
 
@@ -1054,6 +1111,504 @@ void engine_shutdown(Engine* e) {
 
 }  // namespace
 
+namespace {
+// ---------------------------------------------------------------------------
+// Batched slice verification (zg_verify_slices): host side.
+
+// G2 side of seeded params, built on first use: vanishes[d-1][k] =
+// DFT_{w^-1}(coeff)[bitrev_d(k)] * G2 with coeff[0] = tau_c^(N - step), coeff[i] =
+// tau_c^((i-1) step), step = N / 2^d (AMTParams::gen_vanishes,
+// crates/amt/src/prove_params/generate.rs:234-263, on the coset-adjusted
+// powers of from_pp :139-176); high_g2 = tau^(3N) * G2 (high_g2pp has one
+// element, so the coset adjustment multiplies it by w^0).
+void host_dft(std::vector<Fr>& a, const Fr& root) {
+  const size_t n = a.size();
+  for (size_t i = 1, j = 0; i < n; ++i) {  // bit reversal, then iterative DIT
+    size_t bit = n >> 1;
+    for (; j & bit; bit >>= 1) j ^= bit;
+    j ^= bit;
+    if (i < j) std::swap(a[i], a[j]);
+  }
+  for (size_t len = 2; len <= n; len <<= 1) {
+    Fr w = root;
+    for (size_t k = len; k < n; k <<= 1) w = w.sqr();
+    for (size_t i = 0; i < n; i += len) {
+      Fr t = Fr::one();
+      for (size_t k = 0; k < len / 2; ++k) {
+        const Fr u = a[i + k], v = a[i + k + len / 2] * t;
+        a[i + k] = u + v;
+        a[i + k + len / 2] = u - v;
+        t = t * w;
+      }
+    }
+  }
+}
+
+int ensure_g2(zg_ctx* c) {
+  if (c->g2_ready) return 0;
+  if (!c->seeded) return fail(ZG_ERR_PARAMS, "the context has no G2 params");
+  const int ln = c->lr + c->lc;
+  const size_t N = c->N;
+  const Fr tau = tau_from_seed(c->tau_seed);
+  std::vector<Fr> sc;  // canonical scalars: per coset the vanishes, then high_g2
+  for (int cs = 0; cs < 3; ++cs) {
+    const Fr tp = cs ? tau * coset_factor(ln, cs).inverse() : tau;
+    for (int d = 1; d <= c->lr; ++d) {
+      const size_t step = N >> d, sz = (size_t)1 << d;
+      const Fr ts = tp.pow_u64(step);
+      std::vector<Fr> coeff(sz);
+      coeff[0] = tp.pow_u64(N - step);
+      Fr x = Fr::one();
+      for (size_t i = 1; i < sz; ++i) {
+        coeff[i] = x;
+        x = x * ts;
+      }
+      host_dft(coeff, fr_root(d).inverse());
+      // enact = normalize + index_reverse (generate.rs:122-126)
+      for (size_t k = 0; k < sz; ++k) sc.push_back(coeff[host_brev((uint32_t)k, d)].to_canonical());
+    }
+  }
+  sc.push_back(tau.pow_u64((uint64_t)3 * N).to_canonical());
+  const size_t n = sc.size();
+  uint8_t* d_sc = nullptr;
+  G2Aff* d_out = nullptr;
+  ZG_CK(cudaMalloc(&d_sc, n * 32));
+  ZG_CK(cudaMalloc(&d_out, n * sizeof(G2Aff)));
+  ZG_CK(cudaMemcpy(d_sc, sc.data(), n * 32, cudaMemcpyHostToDevice));
+  k_g2_mul<<<nblk(n, 64), 64, 0, c->stream>>>(d_sc, g2_generator(), d_out, (uint32_t)n);
+  std::vector<G2Aff> out(n);
+  cudaError_t e = cudaStreamSynchronize(c->stream);
+  if (e == cudaSuccess) e = cudaMemcpy(out.data(), d_out, n * sizeof(G2Aff), cudaMemcpyDeviceToHost);
+  cudaFree(d_sc);
+  cudaFree(d_out);
+  if (e != cudaSuccess) return fail(ZG_ERR_CUDA, std::string("G2 params: ") + cudaGetErrorString(e));
+  const size_t per = 2 * c->R - 2;
+  for (int cs = 0; cs < 3; ++cs) {
+    c->vanish[cs].assign(out.begin() + cs * per, out.begin() + (cs + 1) * per);
+    c->high_g2[cs] = out[n - 1];
+  }
+  c->g2_ready = true;
+  return 0;
+}
+
+struct G1Pt {
+  G1Aff p;
+  uint8_t inf = 1;
+};
+
+// ark-serialize uncompressed G1 with validation (the point must be on
+// y^2 = x^3 + 3; G1 has cofactor 1)
+bool g1_from_ark(const uint8_t* b, G1Pt* out) {
+  uint8_t fl = 0;
+  Fq x, y;
+  if (!field_from_le(b, &x) || !field_from_le(b + 32, &y, &fl)) return false;
+  if (fl == 3) return false;
+  if (fl == 1) {
+    out->inf = 1;
+    out->p.x = Fq::zero();
+    out->p.y = Fq::zero();
+    return true;
+  }
+  if (!(y * y == x * x * x + Fq::from_u32(3))) return false;
+  out->inf = 0;
+  out->p.x = x;
+  out->p.y = y;
+  return true;
+}
+// EncodeBlobReply.erasure_commitment: x || y as canonical field elements, the
+// affine point at infinity as (0, 0) (grpc/src/service.rs:77-83)
+bool g1_from_reply(const uint8_t* b, G1Pt* out) {
+  bool zero = true;
+  for (int i = 0; i < 64; ++i) zero &= b[i] == 0;
+  out->inf = zero ? 1 : 0;
+  out->p.x = Fq::zero();
+  out->p.y = Fq::zero();
+  return zero || (field_from_le(b, &out->p.x) && field_from_le(b + 32, &out->p.y));
+}
+bool g1_eq(const G1Pt& a, const G1Pt& b) { return a.inf == b.inf && (a.inf || (a.p.x == b.p.x && a.p.y == b.p.y)); }
+
+uint64_t le_u64(const uint8_t* p) {
+  uint64_t v = 0;
+  for (int i = 0; i < 8; ++i) v |= (uint64_t)p[i] << (8 * i);
+  return v;
+}
+
+// one deserialized EncodedSlice (the fields the checks read)
+struct PSlice {
+  const uint8_t* bytes = nullptr;
+  size_t len = 0;
+  uint64_t index = 0, amt_index = 0, row_index = 0, row_len = 0, leaf_index = 0, nmerkle = 0;
+  G1Pt commitment, high;
+  std::vector<G1Pt> comm, quot;
+};
+
+// CanonicalDeserialize of EncodedSlice (derive order, encoder/slice.rs:15-20):
+// every length prefix bounded by the remaining bytes, field elements
+// canonical, points on the curve, no trailing bytes.
+bool parse_slice(const uint8_t* in, size_t len, PSlice* s) {
+  const uint8_t* p = in;
+  const uint8_t* end = in + len;
+  auto left = [&]() { return (size_t)(end - p); };
+  s->bytes = in;
+  s->len = len;
+  if (left() < 16 + 64 + 16) return false;
+  s->index = le_u64(p);
+  s->amt_index = le_u64(p + 8);
+  if (!g1_from_ark(p + 16, &s->commitment)) return false;
+  s->row_index = le_u64(p + 80);
+  s->row_len = le_u64(p + 88);
+  p += 96;
+  if (s->row_len > left() / 32) return false;
+  for (uint64_t i = 0; i < s->row_len; ++i, p += 32) {
+    Fr x;
+    if (!field_from_le(p, &x)) return false;
+  }
+  if (left() < 8) return false;
+  const uint64_t np = le_u64(p);
+  p += 8;
+  if (np > left() / 128) return false;
+  s->comm.resize(np);
+  s->quot.resize(np);
+  for (uint64_t i = 0; i < np; ++i, p += 128)
+    if (!g1_from_ark(p, &s->comm[i]) || !g1_from_ark(p + 64, &s->quot[i])) return false;
+  if (left() < 64 + 96 + 8 || !g1_from_ark(p, &s->high)) return false;
+  p += 64 + 96;
+  const uint64_t nm = le_u64(p);
+  p += 8;
+  if (nm > left() / 32) return false;
+  s->nmerkle = nm;
+  p += 32 * nm;
+  if (left() < 40) return false;
+  s->leaf_index = le_u64(p);
+  p += 40;
+  return p == end;
+}
+
+// SplitMix64 stream of 128-bit coefficients (below r)
+struct Coeffs {
+  uint64_t s;
+  void next(uint32_t w[4]) {
+    for (int k = 0; k < 2; ++k) {
+      const uint64_t x = splitmix64(s);
+      w[2 * k] = (uint32_t)x;
+      w[2 * k + 1] = (uint32_t)(x >> 32);
+    }
+  }
+};
+Fr fr_of_words(const uint32_t w[4]) {
+  Fr x = Fr::zero();
+  for (int i = 0; i < 4; ++i) x.v[i] = w[i];
+  return Fr::from_canonical(x);
+}
+
+// device scratch of one zg_verify_slices call
+struct VerifyRun {
+  zg_ctx* c = nullptr;
+  cudaStream_t s = nullptr;
+  const std::vector<PSlice>* sl = nullptr;
+  G1Pt auth;
+  uint8_t* d_slices = nullptr;  // slices of the batch, stride bytes apart
+  uint64_t stride = 0;
+  std::vector<uint32_t> dpos;   // slice index -> position in d_slices
+  uint8_t* d_scal = nullptr;    // [3][N] canonical scalars of the MSM checks
+  Coeffs rng{0};
+  std::vector<void*> owned;
+  template <class T>
+  T* dev(size_t n) {
+    void* p = nullptr;
+    if (cudaMallocAsync(&p, std::max<size_t>(n, 1) * sizeof(T), s) != cudaSuccess) return nullptr;
+    owned.push_back(p);
+    return static_cast<T*>(p);
+  }
+  void release() {
+    for (void* p : owned) cudaFreeAsync(p, s);
+    owned.clear();
+  }
+};
+
+uint32_t slice_coset(const zg_ctx* c, const PSlice& p) { return (uint32_t)(p.amt_index / c->R); }
+uint32_t slice_bi(const zg_ctx* c, const PSlice& p) { return host_brev((uint32_t)(p.row_index), c->lr); }
+
+// MSM over every coset's basis line with the scalars in d_scal (cosets with
+// present[c]); out[c] on the device
+int verify_msms(VerifyRun& v, const bool present[3], XYZZ* out) {
+  zg_ctx* c = v.c;
+  const uint32_t R = (uint32_t)c->R;
+  for (int cs = 0; cs < 3; ++cs) {
+    if (!present[cs]) continue;
+    k_fb_sort<<<dim3(R, 1), 256, fb_sort_smem_bytes(c->lc), v.s>>>(v.d_scal + (size_t)cs * c->N * 32, c->fb_offs,
+                                                                   c->fb_ents, c->lr, c->lc, 0, 0);
+    FbAccArgs fa;
+    fa.tab = c->line_ptr(cs, c->lr);
+    fa.offs = c->fb_offs;
+    fa.ents = c->fb_ents;
+    fa.outT = c->fb_T;
+    fa.outS = c->fb_S;
+    fa.lr = c->lr;
+    fa.lc = c->lc;
+    fa.lines = 1;
+    fa.tabN = c->N;
+    launch_fb_accum(c, c->msm_product, fa, R, v.s);
+    k_fb_combine<<<nblk(R, 64), 64, 0, v.s>>>(c->fb_T, c->fb_S, c->part, c->lr, 1, R);
+    k_sum_points<<<1, 256, 0, v.s>>>(c->part, R, out + cs);
+  }
+  return check_launch();
+}
+
+// host side: a == b for XYZZ points
+bool xyzz_eq(const XYZZ& a, const XYZZ& b) {
+  XYZZ d = a;
+  d.add(b.neg());
+  return d.is_inf();
+}
+
+// One random linear combination over the AMT checks of `ids` (verify_params.rs:136-211):
+// ok_msm: sum_i a_i (MSM_i + sum_d comm_id - commitment) == O;
+// ok_pair: e(L, g2) prod e(-G, V) prod e(-H_c, high_g2_c) == 1.
+int amt_batch(VerifyRun& v, const std::vector<uint32_t>& ids, bool* ok) {
+  zg_ctx* c = v.c;
+  const std::vector<PSlice>& sl = *v.sl;
+  const int LR = c->lr;
+  const size_t n = ids.size();
+  const uint32_t per = (uint32_t)(2 * c->R - 2);
+  // coefficients
+  std::vector<uint32_t> alpha_w(4 * n), beta_w(4 * n * LR), gamma_w(4 * n);
+  for (size_t j = 0; j < n; ++j) {
+    v.rng.next(&alpha_w[4 * j]);
+    for (int d = 0; d < LR; ++d) v.rng.next(&beta_w[4 * (j * LR + d)]);
+    v.rng.next(&gamma_w[4 * j]);
+  }
+  // MSM check scalars
+  bool present[3] = {false, false, false};
+  std::vector<uint32_t> h_pos(n), h_cos(n), h_bi(n);
+  std::vector<Fr> h_alpha(n);
+  Fr asum[3] = {Fr::zero(), Fr::zero(), Fr::zero()}, gsum[3] = {Fr::zero(), Fr::zero(), Fr::zero()};
+  for (size_t j = 0; j < n; ++j) {
+    const PSlice& p = sl[ids[j]];
+    h_pos[j] = v.dpos[ids[j]];
+    h_cos[j] = slice_coset(c, p);
+    h_bi[j] = slice_bi(c, p);
+    h_alpha[j] = fr_of_words(&alpha_w[4 * j]);
+    present[h_cos[j]] = true;
+    asum[h_cos[j]] = asum[h_cos[j]] + h_alpha[j];
+    gsum[h_cos[j]] = gsum[h_cos[j]] + fr_of_words(&gamma_w[4 * j]);
+  }
+  uint32_t* d_pos = v.dev<uint32_t>(n);
+  uint32_t* d_cos = v.dev<uint32_t>(n);
+  uint32_t* d_bi = v.dev<uint32_t>(n);
+  Fr* d_alpha = v.dev<Fr>(n);
+  if (!d_pos || !d_cos || !d_bi || !d_alpha) return fail(ZG_ERR_CUDA, "verify: device allocation failed");
+  ZG_CK(cudaMemcpyAsync(d_pos, h_pos.data(), 4 * n, cudaMemcpyHostToDevice, v.s));
+  ZG_CK(cudaMemcpyAsync(d_cos, h_cos.data(), 4 * n, cudaMemcpyHostToDevice, v.s));
+  ZG_CK(cudaMemcpyAsync(d_bi, h_bi.data(), 4 * n, cudaMemcpyHostToDevice, v.s));
+  ZG_CK(cudaMemcpyAsync(d_alpha, h_alpha.data(), n * sizeof(Fr), cudaMemcpyHostToDevice, v.s));
+  for (int cs = 0; cs < 3; ++cs)
+    if (present[cs]) ZG_CK(cudaMemsetAsync(v.d_scal + (size_t)cs * c->N * 32, 0, c->N * 32, v.s));
+  k_verify_scalars<<<(unsigned)n, 256, 0, v.s>>>(v.d_slices, v.stride, d_pos, c->lc, d_cos, d_bi, d_alpha, v.d_scal,
+                                                 c->N * 32);
+  XYZZ* d_msm = v.dev<XYZZ>(3);
+  if (!d_msm) return fail(ZG_ERR_CUDA, "verify: device allocation failed");
+  int rc = verify_msms(v, present, d_msm);
+  if (rc) return rc;
+  // weighted G1 terms: [L: comm (beta), high (gamma)] [G: quot (beta), by group] [D: comm (alpha)]
+  std::vector<uint32_t> gkey(n * LR);
+  std::vector<uint32_t> gcount((size_t)3 * per, 0);
+  for (size_t j = 0; j < n; ++j)
+    for (int d = 0; d < LR; ++d) {
+      const uint32_t vi = (h_bi[j] >> (LR - 1 - d)) ^ 1u;
+      gkey[j * LR + d] = h_cos[j] * per + ((2u << d) - 2) + vi;
+      ++gcount[gkey[j * LR + d]];
+    }
+  std::vector<uint32_t> gid((size_t)3 * per, UINT32_MAX), goff(1, 0);
+  for (size_t k = 0; k < gid.size(); ++k)
+    if (gcount[k]) {
+      gid[k] = (uint32_t)goff.size() - 1;
+      goff.push_back(goff.back() + gcount[k]);
+    }
+  const uint32_t ng = (uint32_t)goff.size() - 1;
+  const size_t nL = n * (LR + 1), nG = n * LR, nD = n * LR, nt = nL + nG + nD;
+  std::vector<G1Aff> tp(nt);
+  std::vector<uint8_t> tinf(nt);
+  std::vector<uint32_t> tsc(4 * nt);
+  std::vector<uint32_t> fill(goff.begin(), goff.end() - 1);
+  auto put = [&](size_t t, const G1Pt& q, const uint32_t* w) {
+    tp[t] = q.p;
+    tinf[t] = q.inf;
+    for (int k = 0; k < 4; ++k) tsc[4 * t + k] = w[k];
+  };
+  for (size_t j = 0; j < n; ++j) {
+    const PSlice& p = sl[ids[j]];
+    for (int d = 0; d < LR; ++d) {
+      put(j * (LR + 1) + d, p.comm[d], &beta_w[4 * (j * LR + d)]);
+      put(nL + fill[gid[gkey[j * LR + d]]]++, p.quot[d], &beta_w[4 * (j * LR + d)]);
+      put(nL + nG + j * LR + d, p.comm[d], &alpha_w[4 * j]);
+    }
+    put(j * (LR + 1) + LR, p.high, &gamma_w[4 * j]);
+  }
+  G1Aff* d_tp = v.dev<G1Aff>(nt);
+  uint8_t* d_tinf = v.dev<uint8_t>(nt);
+  uint32_t* d_tsc = v.dev<uint32_t>(4 * nt);
+  XYZZ* d_terms = v.dev<XYZZ>(nt);
+  uint32_t* d_goff = v.dev<uint32_t>(goff.size());
+  // pairing inputs: [0] L, [1..ng] G_g, then H_c per present coset; extra: D sum, A, H scalars
+  const uint32_t npair = 1 + ng + (present[0] + present[1] + present[2]);
+  XYZZ* d_pin = v.dev<XYZZ>(npair + 2);  // + D sum, A = (sum alpha) commitment
+  if (!d_tp || !d_tinf || !d_tsc || !d_terms || !d_goff || !d_pin) return fail(ZG_ERR_CUDA, "verify: allocation");
+  ZG_CK(cudaMemcpyAsync(d_tp, tp.data(), nt * sizeof(G1Aff), cudaMemcpyHostToDevice, v.s));
+  ZG_CK(cudaMemcpyAsync(d_tinf, tinf.data(), nt, cudaMemcpyHostToDevice, v.s));
+  ZG_CK(cudaMemcpyAsync(d_tsc, tsc.data(), 16 * nt, cudaMemcpyHostToDevice, v.s));
+  ZG_CK(cudaMemcpyAsync(d_goff, goff.data(), 4 * goff.size(), cudaMemcpyHostToDevice, v.s));
+  k_g1_mul_words<<<nblk(nt, 128), 128, 0, v.s>>>(d_tp, d_tinf, d_tsc, 4, d_terms, (uint32_t)nt);
+  k_sum_points<<<1, 256, 0, v.s>>>(d_terms, (uint32_t)nL, d_pin);
+  k_seg_sum<<<nblk(ng, 128), 128, 0, v.s>>>(d_terms + nL, d_goff, d_pin + 1, ng);
+  k_sum_points<<<1, 256, 0, v.s>>>(d_terms + nL + nG, (uint32_t)nD, d_pin + npair);
+  // full-size multiples of the commitment: H_c = (sum gamma over c) C, A = (sum alpha) C
+  std::vector<uint32_t> big;
+  std::vector<G1Aff> bigp;
+  Fr atot = asum[0] + asum[1] + asum[2];
+  for (int cs = 0; cs < 4; ++cs) {
+    if (cs < 3 && !present[cs]) continue;
+    const Fr k = (cs < 3 ? gsum[cs] : atot).to_canonical();
+    big.insert(big.end(), k.v, k.v + 8);
+    bigp.push_back(v.auth.p);
+  }
+  const uint32_t nb = (uint32_t)bigp.size();
+  G1Aff* d_bp = v.dev<G1Aff>(nb);
+  uint8_t* d_binf = v.dev<uint8_t>(nb);
+  uint32_t* d_bsc = v.dev<uint32_t>(8 * nb);
+  if (!d_bp || !d_binf || !d_bsc) return fail(ZG_ERR_CUDA, "verify: allocation");
+  std::vector<uint8_t> binf(nb, v.auth.inf);
+  ZG_CK(cudaMemcpyAsync(d_bp, bigp.data(), nb * sizeof(G1Aff), cudaMemcpyHostToDevice, v.s));
+  ZG_CK(cudaMemcpyAsync(d_binf, binf.data(), nb, cudaMemcpyHostToDevice, v.s));
+  ZG_CK(cudaMemcpyAsync(d_bsc, big.data(), 32 * nb, cudaMemcpyHostToDevice, v.s));
+  // H_c land after the groups, A after the D sum
+  k_g1_mul_words<<<1, 128, 0, v.s>>>(d_bp, d_binf, d_bsc, 8, d_pin + 1 + ng, nb - 1);
+  k_g1_mul_words<<<1, 128, 0, v.s>>>(d_bp + nb - 1, d_binf + nb - 1, d_bsc + 8 * (nb - 1), 8, d_pin + npair + 1, 1);
+  // MSM check on the host
+  XYZZ hm[3], hd[2];
+  ZG_CK(cudaMemcpyAsync(hm, d_msm, sizeof(hm), cudaMemcpyDeviceToHost, v.s));
+  ZG_CK(cudaMemcpyAsync(hd, d_pin + npair, sizeof(hd), cudaMemcpyDeviceToHost, v.s));
+  // pairing: Miller loops on the device
+  std::vector<G2Aff> q(npair);
+  std::vector<uint8_t> neg(npair, 1);
+  q[0] = g2_generator();
+  neg[0] = 0;
+  for (size_t k = 0; k < gid.size(); ++k)
+    if (gid[k] != UINT32_MAX) q[1 + gid[k]] = c->vanish[k / per][k % per];
+  for (int cs = 0, h = 0; cs < 3; ++cs)
+    if (present[cs]) q[1 + ng + h++] = c->high_g2[cs];
+  G2Aff* d_q = v.dev<G2Aff>(npair);
+  uint8_t* d_neg = v.dev<uint8_t>(npair);
+  G1Aff* d_pa = v.dev<G1Aff>(npair);
+  uint8_t* d_pinf = v.dev<uint8_t>(npair);
+  Fq12* d_f = v.dev<Fq12>(npair);
+  Fq12* d_part = v.dev<Fq12>(128);
+  if (!d_q || !d_neg || !d_pa || !d_pinf || !d_f || !d_part) return fail(ZG_ERR_CUDA, "verify: allocation");
+  ZG_CK(cudaMemcpyAsync(d_q, q.data(), npair * sizeof(G2Aff), cudaMemcpyHostToDevice, v.s));
+  ZG_CK(cudaMemcpyAsync(d_neg, neg.data(), npair, cudaMemcpyHostToDevice, v.s));
+  k_pairing_inputs<<<nblk(npair, 128), 128, 0, v.s>>>(d_pin, d_neg, d_pa, d_pinf, npair);
+  k_miller<<<nblk(npair, 64), 64, 0, v.s>>>(d_pa, d_pinf, d_q, d_f, npair);
+  k_fq12_partial<<<1, 128, 0, v.s>>>(d_f, npair, d_part);
+  std::vector<Fq12> part(128);
+  ZG_CK(cudaMemcpyAsync(part.data(), d_part, 128 * sizeof(Fq12), cudaMemcpyDeviceToHost, v.s));
+  if ((rc = check_launch())) return rc;
+  ZG_CK(cudaStreamSynchronize(v.s));
+  XYZZ left = XYZZ::inf();
+  for (int cs = 0; cs < 3; ++cs)
+    if (present[cs]) left.add(hm[cs]);
+  left.add(hd[0]);
+  const bool ok_msm = xyzz_eq(left, hd[1]);
+  Fq12 f = Fq12::one();
+  for (auto& x : part) f = f * x;
+  const bool ok_pair = final_exp(f).is_one();
+  *ok = ok_msm && ok_pair;
+  return 0;
+}
+
+// host pairing equality e(a, b) == e(c, d)
+bool host_pairing_eq(const G1Pt& a, const G2Aff& b, const G1Pt& cc, const G2Aff& d) {
+  G1Aff cn = cc.p;
+  cn.y = -cn.y;
+  return final_exp(miller_tate(a.p, a.inf != 0, b) * miller_tate(cn, cc.inf != 0, d)).is_one();
+}
+
+// verify_amt_proof for one slice in the reference's order (KZG from the
+// deepest layer, MSM consistency, low-degree test); sub / kzg d as the
+// reference's AmtProofError
+int amt_single(VerifyRun& v, uint32_t id, int* sub, int64_t* kzg_d) {
+  zg_ctx* c = v.c;
+  const PSlice& p = (*v.sl)[id];
+  const uint32_t cs = slice_coset(c, p), bi = slice_bi(c, p);
+  const int LR = c->lr;
+  const uint32_t per = (uint32_t)(2 * c->R - 2);
+  (void)per;
+  for (int d = LR - 1; d >= 0; --d) {
+    const uint32_t vi = (bi >> (LR - 1 - d)) ^ 1u;
+    const G2Aff& V = c->vanish[cs][((2u << d) - 2) + vi];
+    if (!host_pairing_eq(p.comm[d], g2_generator(), p.quot[d], V)) {
+      *sub = 2;
+      *kzg_d = d;
+      return 0;
+    }
+  }
+  // MSM consistency: sum_d comm_d + MSM(basis[bi C ..], data) == commitment
+  bool present[3] = {false, false, false};
+  present[cs] = true;
+  uint32_t* d_pos = v.dev<uint32_t>(1);
+  uint32_t* d_cos = v.dev<uint32_t>(1);
+  uint32_t* d_bi = v.dev<uint32_t>(1);
+  Fr* d_alpha = v.dev<Fr>(1);
+  XYZZ* d_msm = v.dev<XYZZ>(3);
+  if (!d_pos || !d_cos || !d_bi || !d_alpha || !d_msm) return fail(ZG_ERR_CUDA, "verify: allocation");
+  const Fr one = Fr::one();
+  ZG_CK(cudaMemcpyAsync(d_pos, &v.dpos[id], 4, cudaMemcpyHostToDevice, v.s));
+  ZG_CK(cudaMemcpyAsync(d_cos, &cs, 4, cudaMemcpyHostToDevice, v.s));
+  ZG_CK(cudaMemcpyAsync(d_bi, &bi, 4, cudaMemcpyHostToDevice, v.s));
+  ZG_CK(cudaMemcpyAsync(d_alpha, &one, sizeof(Fr), cudaMemcpyHostToDevice, v.s));
+  ZG_CK(cudaMemsetAsync(v.d_scal + (size_t)cs * c->N * 32, 0, c->N * 32, v.s));
+  k_verify_scalars<<<1, 256, 0, v.s>>>(v.d_slices, v.stride, d_pos, c->lc, d_cos, d_bi, d_alpha, v.d_scal, c->N * 32);
+  int rc = verify_msms(v, present, d_msm);
+  if (rc) return rc;
+  XYZZ m;
+  ZG_CK(cudaMemcpyAsync(&m, d_msm + cs, sizeof(XYZZ), cudaMemcpyDeviceToHost, v.s));
+  ZG_CK(cudaStreamSynchronize(v.s));
+  for (int d = 0; d < LR; ++d)
+    if (!p.comm[d].inf) m.add_affine(p.comm[d].p.x, p.comm[d].p.y);
+  XYZZ com = XYZZ::inf();
+  if (!v.auth.inf) com.add_affine(v.auth.p.x, v.auth.p.y);
+  if (!xyzz_eq(m, com)) {
+    *sub = 3;
+    return 0;
+  }
+  if (!host_pairing_eq(p.high, g2_generator(), v.auth, c->high_g2[cs])) {
+    *sub = 4;
+    return 0;
+  }
+  *sub = -1;
+  return 0;
+}
+
+// bisect a failing batch down to its failing slices
+int amt_resolve(VerifyRun& v, const std::vector<uint32_t>& ids, std::vector<int>& sub, std::vector<int64_t>& kd) {
+  if (ids.empty()) return 0;
+  if (ids.size() == 1) {
+    int s = -1;
+    int64_t d = 0;
+    int rc = amt_single(v, ids[0], &s, &d);
+    sub[ids[0]] = s;
+    kd[ids[0]] = d;
+    return rc;
+  }
+  bool ok = false;
+  int rc = amt_batch(v, ids, &ok);
+  if (rc || ok) return rc;
+  std::vector<uint32_t> a(ids.begin(), ids.begin() + ids.size() / 2), b(ids.begin() + ids.size() / 2, ids.end());
+  if ((rc = amt_resolve(v, a, sub, kd))) return rc;
+  return amt_resolve(v, b, sub, kd);
+}
+
+}  // namespace
+
 extern "C" {
 
 const char* zg_last_error(void) { return g_err.c_str(); }
@@ -1104,7 +1659,11 @@ int zg_ctx_create(const zg_config* cfg, zg_ctx** out) {
     return bail(fail(ZG_ERR_CUDA, "cannot allocate params"));
   if ((rc = alloc_blob_buffers(c))) return bail(rc);
   if (cfg->params_dir && cfg->params_dir[0]) rc = load_mont_params(c, cfg->params_dir);
-  else rc = build_seeded_params(c, cfg->tau_seed);
+  else {
+    rc = build_seeded_params(c, cfg->tau_seed);
+    c->seeded = true;
+    c->tau_seed = cfg->tau_seed;
+  }
   if (rc) return bail(rc);
   if (c->fb) {
     const uint64_t nl = (uint64_t)3 * c->L;
@@ -1379,6 +1938,138 @@ int zg_ctx_param_points(zg_ctx* c, int coset, int line, size_t first, size_t cou
   std::lock_guard<std::mutex> g(c->mu);
   ZG_CK(cudaSetDevice(c->device));
   ZG_CK(cudaMemcpy(host_out, c->line_ptr(coset, line) + first, bytes, cudaMemcpyDeviceToHost));
+  return ZG_OK;
+}
+
+int zg_verify_slices(zg_ctx* c, const uint8_t* const* slices, const size_t* lens, size_t n, const uint8_t* commitment,
+                     const uint8_t* storage_root, uint64_t seed, int32_t* codes, int64_t* details) {
+  if (!c || !commitment || !storage_root || (n && (!slices || !lens || !codes)))
+    return fail(ZG_ERR_INVALID_ARG, "null argument");
+  if (!c->fb) return fail(ZG_ERR_INVALID_ARG, "zg_verify_slices needs the fixed-base tables (msm_window_bits 0 or 11)");
+  std::lock_guard<std::mutex> g(c->mu);
+  ZG_CK(cudaSetDevice(c->device));
+  int rc = ensure_g2(c);
+  if (rc) return rc;
+  const uint64_t R = c->R, C = c->C;
+  std::vector<PSlice> sl(n);
+  std::vector<int64_t> det(4 * n, 0);
+  for (size_t i = 0; i < n; ++i) codes[i] = 0;
+  VerifyRun v;
+  v.c = c;
+  v.s = c->stream;
+  v.sl = &sl;
+  if (!seed) {
+    std::random_device rd;
+    seed = ((uint64_t)rd() << 32) ^ rd();
+  }
+  v.rng.s = seed;
+  const bool auth_ok = g1_from_reply(commitment, &v.auth);
+  // deserialization and the structural checks, in the reference's order
+  // (EncodedSlice::verify, encoder/slice.rs:73-95; EncodedSliceAMT::verify,
+  // amt/slice.rs:53-103; verify_amt_proof's length checks, verify_params.rs:147-160)
+  std::vector<uint32_t> batch;
+  size_t maxlen = 0;
+  for (size_t i = 0; i < n; ++i) {
+    int64_t* d = &det[4 * i];
+    PSlice& p = sl[i];
+    if (!auth_ok || !slices[i] || !parse_slice(slices[i], lens[i], &p)) { codes[i] = 30; continue; }
+    const uint64_t coset = p.amt_index / R, local = p.amt_index % R;
+    if (p.index != p.amt_index) { codes[i] = 1; d[1] = (int64_t)p.index; d[2] = (int64_t)p.amt_index; }
+    else if (p.index != p.leaf_index) { codes[i] = 2; d[1] = (int64_t)p.index; d[2] = (int64_t)p.leaf_index; }
+    else if (!g1_eq(p.commitment, v.auth)) codes[i] = 10;
+    else if (p.row_len != C) { codes[i] = 11; d[1] = (int64_t)p.row_len; d[2] = (int64_t)C; }
+    else if (p.amt_index >= 3 * R) { codes[i] = 12; d[1] = (int64_t)p.amt_index; d[2] = (int64_t)(3 * R); }
+    else if (local != p.row_index) { codes[i] = 13; d[1] = (int64_t)coset; d[2] = (int64_t)local; d[3] = (int64_t)p.row_index; }
+    else if (p.comm.size() != (size_t)c->lr) {
+      // proof depth: batch = N >> depth must equal the row length
+      codes[i] = 14;
+      d[1] = (int64_t)coset;
+      d[2] = (int64_t)p.row_index;
+      const size_t depth = p.comm.size();
+      d[0] = (depth >= 63 || (c->N >> depth) != C) ? 0 : 1;
+    } else {
+      batch.push_back((uint32_t)i);
+      maxlen = std::max(maxlen, lens[i]);
+    }
+  }
+  if (!batch.empty()) {
+    const size_t nb = batch.size();
+    v.stride = (maxlen + 15) & ~(size_t)15;
+    v.dpos.assign(n, 0);
+    uint8_t* stage = (uint8_t*)pinned_get(nb * v.stride);
+    if (!stage) return fail(ZG_ERR_CUDA, "cannot allocate pinned staging");
+    std::vector<uint32_t> nproof(nb);
+    for (size_t j = 0; j < nb; ++j) {
+      const uint32_t i = batch[j];
+      v.dpos[i] = (uint32_t)j;
+      memcpy(stage + j * v.stride, slices[i], lens[i]);
+      nproof[j] = (uint32_t)sl[i].nmerkle;
+    }
+    v.d_slices = v.dev<uint8_t>(nb * v.stride);
+    v.d_scal = v.dev<uint8_t>(3 * c->N * 32);
+    uint32_t* d_np = v.dev<uint32_t>(nb);
+    uint8_t* d_root = v.dev<uint8_t>(32);
+    int32_t* d_mcode = v.dev<int32_t>(nb);
+    rc = (!v.d_slices || !v.d_scal || !d_np || !d_root || !d_mcode) ? fail(ZG_ERR_CUDA, "verify: allocation") : 0;
+    std::vector<int32_t> mcode(nb, 0);
+    std::vector<int> sub(n, -1);
+    std::vector<int64_t> kd(n, 0);
+    if (!rc) {
+      cudaStreamWaitEvent(v.s, c->done, 0);
+      cudaMemcpyAsync(v.d_slices, stage, nb * v.stride, cudaMemcpyHostToDevice, v.s);
+      cudaMemcpyAsync(d_np, nproof.data(), 4 * nb, cudaMemcpyHostToDevice, v.s);
+      cudaMemcpyAsync(d_root, storage_root, 32, cudaMemcpyHostToDevice, v.s);
+      k_verify_merkle<<<(unsigned)nb, 128, 0, v.s>>>(v.d_slices, v.stride, c->lr, c->lc, d_np, d_root, d_mcode);
+      cudaMemcpyAsync(mcode.data(), d_mcode, 4 * nb, cudaMemcpyDeviceToHost, v.s);
+      rc = check_launch();
+    }
+    // the AMT checks: one random linear combination per round, bisected down
+    // to the failing slices when it fails. Slices naming the same (coset, row)
+    // go to different rounds: their MSM scalars share one place of the
+    // coset's scalar vector.
+    std::vector<std::vector<uint32_t>> rounds;
+    {
+      std::map<uint64_t, uint32_t> seen;
+      for (uint32_t i : batch) {
+        const uint32_t k = seen[sl[i].amt_index]++;
+        if (k >= rounds.size()) rounds.emplace_back();
+        rounds[k].push_back(i);
+      }
+    }
+    for (size_t r = 0; !rc && r < rounds.size(); ++r) {
+      const std::vector<uint32_t>& ids = rounds[r];
+      bool ok = false;
+      rc = amt_batch(v, ids, &ok);
+      if (!rc && !ok) {
+        const size_t h = ids.size() / 2;
+        std::vector<uint32_t> a(ids.begin(), ids.begin() + h), b(ids.begin() + h, ids.end());
+        if (ids.size() == 1) rc = amt_resolve(v, ids, sub, kd);
+        else if (!(rc = amt_resolve(v, a, sub, kd))) rc = amt_resolve(v, b, sub, kd);
+      }
+    }
+    if (!rc) rc = cudaStreamSynchronize(v.s) == cudaSuccess ? 0 : fail(ZG_ERR_CUDA, "verify: stream failed");
+    if (!rc) cudaEventRecord(c->done, v.s);
+    v.release();
+    cudaStreamSynchronize(v.s);
+    pinned_put(stage, nb * v.stride);
+    if (rc) return rc;
+    for (size_t j = 0; j < nb; ++j) {
+      const uint32_t i = batch[j];
+      int64_t* d = &det[4 * i];
+      if (sub[i] >= 0) {
+        codes[i] = 14;
+        d[0] = sub[i];
+        d[1] = (int64_t)(sl[i].amt_index / R);
+        d[2] = (int64_t)sl[i].row_index;
+        d[3] = sub[i] == 2 ? kd[i] : 0;
+      } else if (mcode[j]) {
+        codes[i] = mcode[j];
+        if (mcode[j] == 22) { d[1] = (int64_t)sl[i].leaf_index; d[2] = (int64_t)(3 * R); }
+        if (mcode[j] == 23 || mcode[j] == 24) d[1] = (int64_t)sl[i].leaf_index;
+      }
+    }
+  }
+  if (details) memcpy(details, det.data(), det.size() * sizeof(int64_t));
   return ZG_OK;
 }
 

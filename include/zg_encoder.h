@@ -190,6 +190,45 @@ int zg_encode_batch(zg_ctx* ctx, size_t n, const uint8_t* const* data, const siz
 int zg_ctx_msm(zg_ctx* ctx, uint32_t coset, uint32_t line, const void* d_scalars, size_t n, void* d_out,
                void* stream);
 
+/* Batched EncodedSlice::verify (crates/encoder/src/encoder/slice.rs:73-95) on
+ * the GPU. slices[i] (host memory, lens[i] bytes) is one ark-serialized
+ * EncodedSlice of a blob, checked against the blob's erasure commitment (the
+ * 64 bytes of zg_reply_erasure_commitment: x || y canonical little-endian,
+ * all zero for the point at infinity) and storage root (32 B).
+ * codes[i] receives the verdict in the reference's check order:
+ *   ZG_V_OK, ZG_V_UNMATCHED_AMT_INDEX, ZG_V_UNMATCHED_MERKLE_INDEX (VerifierError),
+ *   ZG_V_AMT_INCORRECT_COMMITMENT .. ZG_V_AMT_INCORRECT_PROOF (AmtSignerError),
+ *   ZG_V_MERKLE_INCORRECT_ROOT .. ZG_V_MERKLE_INCORRECT_PROOF (MerkleSignerError),
+ *   ZG_V_DESERIALIZE (the bytes are not a valid EncodedSlice);
+ * details (4 int64 per slice, may be NULL) the variant's fields: [0] the
+ * AmtProofError of ZG_V_AMT_INCORRECT_PROOF (0 UnexpectedDataLength,
+ * 1 IncorrectPosition, 2 KzgError(d), 3 InconsistentCommitment,
+ * 4 FailedLowDegreeTest), [1..3] the variant's integers (indices and sizes,
+ * d of KzgError in [3]). The AMT pairing and MSM checks of all slices are
+ * folded into random linear combinations (the reference's DeferredVerifier,
+ * crates/amt/src/deferred_verification.rs:67-146) with 128-bit coefficients
+ * from `seed` (0: from the OS), and bisected down to single slices when a
+ * combination fails, so every code is the one EncodedSlice::verify returns
+ * (up to the 2^-128 chance of a false accept). Needs the fixed-base tables.
+ * Returns ZG_OK once every slice has its verdict. */
+#define ZG_V_OK 0
+#define ZG_V_UNMATCHED_AMT_INDEX 1
+#define ZG_V_UNMATCHED_MERKLE_INDEX 2
+#define ZG_V_AMT_INCORRECT_COMMITMENT 10
+#define ZG_V_AMT_INCORRECT_ROW_SIZE 11
+#define ZG_V_AMT_ROW_INDEX_OVERFLOW 12
+#define ZG_V_AMT_UNMATCHED_COSET_INDEX 13
+#define ZG_V_AMT_INCORRECT_PROOF 14
+#define ZG_V_MERKLE_INCORRECT_ROOT 20
+#define ZG_V_MERKLE_INCORRECT_SIZE 21
+#define ZG_V_MERKLE_ROW_INDEX_OVERFLOW 22
+#define ZG_V_MERKLE_INCORRECT_LOCAL_ROOT 23
+#define ZG_V_MERKLE_INCORRECT_PROOF 24
+#define ZG_V_DESERIALIZE 30
+int zg_verify_slices(zg_ctx* ctx, const uint8_t* const* slices, const size_t* lens, size_t n,
+                     const uint8_t* commitment, const uint8_t* storage_root, uint64_t seed, int32_t* codes,
+                     int64_t* details);
+
 /* LightEncodedSlice (crates/encoder/src/encoder/light_slice.rs:11-79), host
  * byte conversions of the ark-serialized layouts (no device work).
  * from_slice: LightEncodedSlice::from_slice / EncodedSlice::into_light_slice;

@@ -128,26 +128,7 @@ def test_erasure_encoding(oracle):
 
 
 # ---- verify and the reference's fault-injection table ------------------------
-def slice_layout(lr, lc):
-    C = 1 << lc
-    a = 96 + 32 * C
-    h = a + 8 + 128 * lr
-    m = h + 64
-    t = m + 104 + 32 * lr
-    return {"row": 96, "proof": a + 8, "high": h, "merkle": m, "mproof": m + 104, "leaf_index": t,
-            "leaf": t + 8, "end": t + 40}
-
-
-def parse_g1(b):
-    if b[63] & 0x40:
-        return None
-    y = bytearray(b[32:])
-    y[31] &= 0x3F
-    return int.from_bytes(b[:32], "little"), int.from_bytes(bytes(y), "little")
-
-
-def bump(h):  # H256::from_low_u64_be(H256(h).to_low_u64_be() + 1)
-    return bytes(24) + ((int.from_bytes(h[24:], "big") + 1) & ((1 << 64) - 1)).to_bytes(8, "big")
+from slice_faults import fault_cases  # noqa: E402
 
 
 @pytest.fixture(scope="module")
@@ -172,51 +153,13 @@ def test_fault_injection_error_codes(oracle, blob_4x6, index):
     amt/blob.rs:61-96, merkle/blob.rs:60-106): each corruption yields exactly
     the reference's VerifierError variant."""
     op, ob, slices = blob_4x6
-    R = 16
-    lay = slice_layout(4, 6)
-    s = slices[index]
-    coset, local = divmod(index, R)
     com, root = ob.commitment(), ob.file_root()
-
-    def check(buf, code, sub=0, a=0, b=0, c=0):
+    for buf, code, sub, a, b, c in fault_cases(slices, index, 4, 6):
         rc, det = oracle.verify(op, bytes(buf), com, root)
         assert rc == code, (index, rc, det)
-        if code in (zgo.V_AMT_INCORRECT_PROOF,):
+        if code == zgo.V_AMT_INCORRECT_PROOF:
             assert det[0] == sub
         assert det[1:] == [a, b, c], (index, rc, det)
-
-    u64 = lambda v: v.to_bytes(8, "little")
-    check(u64(index + 1) + s[8:], zgo.V_UNMATCHED_AMT_INDEX, a=index + 1, b=index)
-    if index < 3 * R - 1:
-        nxt = slices[index + 1]
-        check(s[:8] + nxt[8:lay["merkle"]] + s[lay["merkle"]:], zgo.V_UNMATCHED_AMT_INDEX, a=index, b=index + 1)
-        check(s[:lay["merkle"]] + nxt[lay["merkle"]:], zgo.V_UNMATCHED_MERKLE_INDEX, a=index, b=index + 1)
-    # AMT: WrongRow
-    row0 = (int.from_bytes(s[96:128], "little") + 1) % R_MOD
-    check(s[:96] + row0.to_bytes(32, "little") + s[128:], zgo.V_AMT_INCORRECT_PROOF, sub=zgo.P_INCONSISTENT,
-          a=coset, b=local)
-    # AMT: WrongIndex (row.index += 1)
-    check(s[:80] + u64(local + 1) + s[88:], zgo.V_AMT_UNMATCHED_COSET_INDEX, a=coset, b=local, c=local + 1)
-    # AMT: WrongCommitment (commitment + G1)
-    bad_com = mg.ser_g1(mg.g1_add(parse_g1(s[16:80]), mg.G1))
-    check(s[:16] + bad_com + s[80:], zgo.V_AMT_INCORRECT_COMMITMENT)
-    # AMT: IncorrectHighCommitment (high + G1)
-    h = lay["high"]
-    bad_high = mg.ser_g1(mg.g1_add(parse_g1(s[h:h + 64]), mg.G1))
-    check(s[:h] + bad_high + s[h + 64:], zgo.V_AMT_INCORRECT_PROOF, sub=zgo.P_LDT, a=coset, b=local)
-    # Merkle: WrongIndex (leaf_index += 1)
-    li = lay["leaf_index"]
-    check(s[:li] + u64(index + 1) + s[li + 8:], zgo.V_UNMATCHED_MERKLE_INDEX, a=index, b=index + 1)
-    # Merkle: WrongLocalRoot
-    lf = lay["leaf"]
-    check(s[:lf] + bump(s[lf:lf + 32]), zgo.V_MERKLE_INCORRECT_LOCAL_ROOT, a=index)
-    # Merkle: WrongProof (proof[0])
-    mp = lay["mproof"]
-    check(s[:mp] + bump(s[mp:mp + 32]) + s[mp + 32:], zgo.V_MERKLE_INCORRECT_PROOF, a=index)
-    # Merkle: WrongRoot (every root)
-    m = lay["merkle"]
-    roots = b"".join(bump(s[m + 32 * k:m + 32 * k + 32]) for k in range(3))
-    check(s[:m] + roots + s[m + 96:], zgo.V_MERKLE_INCORRECT_ROOT)
 
 
 def test_too_large_blob(oracle):
