@@ -107,6 +107,8 @@ def parse():
     ap.add_argument("--serve-requests", type=int, default=16, help="requests in the serving sample (0 = skip)")
     ap.add_argument("--serve-plain", action="store_true",
                     help="also serve the same arrivals through the blocking per-blob path")
+    ap.add_argument("--verify-sample", type=int, default=4,
+                    help="slices of the CPU verification sample (0 = skip the verification measurement)")
     ap.add_argument("--micro", action="store_true",
                     help="kernel microbenchmarks instead of the blob benchmark: single MSMs of 2^16/2^18/2^20 "
                          "points (uniform and blob-like scalars), NTTs (1024 x 2^10, 64 x 2^14, 1 x 2^20; "
@@ -636,6 +638,37 @@ def main():
         if args.serve_plain:
             extra["serving"].append(serving_run(pkg, params, pipe, h_ptr, full, recs, args.serve_rate,
                                                 args.serve_requests, 5, plain=True))
+
+    # batched verification of every slice of one blob (EncodedSlice::verify for
+    # 3072 slices through zg_verify_slices), beside the oracle's per-slice
+    # verifier on a sample
+    if world == 1 and args.verify_sample > 0:
+        rep = pkg.EncoderService(params).process_data(payload.tobytes(), True)
+        times = []
+        for k in range(2):
+            t0 = time.perf_counter()
+            codes, _ = pkg.verify_slices(params, rep.encoded_slice, rep.erasure_commitment, rep.storage_root,
+                                         seed=11 + k)
+            times.append(time.perf_counter() - t0)
+        ver = {"slices": len(rep.encoded_slice), "seconds": min(times),
+               "slices_per_s": len(rep.encoded_slice) / min(times), "all_ok": all(c == 0 for c in codes),
+               "path": "zg_verify_slices (host slice bytes in, verdicts out; GPU Merkle paths, MSM and Miller "
+                       "loops, host final exponentiation)"}
+        if not args.no_cpu_baseline:
+            sys.path.insert(0, os.path.join(ROOT, "tests"))
+            import zgo
+            o = zgo.Oracle()
+            basis = b"".join(params.param_line(cs, LOG_ROW) for cs in range(3))
+            vp = o.verify_params(LOG_ROW, LOG_COL, PARAM_SEED, basis)
+            ids = list(range(0, 3 * R, max(1, 3 * R // args.verify_sample)))[:args.verify_sample]
+            t0 = time.perf_counter()
+            for i in ids:
+                o.verify(vp, rep.encoded_slice[i], rep.erasure_commitment, rep.storage_root)
+            dt = time.perf_counter() - t0
+            ver["cpu_oracle"] = {"slices": len(ids), "seconds": dt, "slices_per_s": len(ids) / dt,
+                                 "cores": o.L.zgo_num_threads(),
+                                 "note": "C++ restatement of EncodedSlice::verify, one slice at a time"}
+        extra["verify"] = ver
 
     hbm, hbm_tag = measured_peaks()
     t_msm = phases["msm"] / 1000.0
