@@ -113,6 +113,12 @@ def parse():
                     help="kernel microbenchmarks instead of the blob benchmark: single MSMs of 2^16/2^18/2^20 "
                          "points (uniform and blob-like scalars), NTTs (1024 x 2^10, 64 x 2^14, 1 x 2^20; "
                          "forward, inverse, coset), Keccak Merkle over 3072 x 1024 x 32 B")
+    ap.add_argument("--tuning", default="",
+                    help="PRODUCT,COLS,THREADS (e.g. hybrid,1,256): use these kernel choices instead of autotuning "
+                         "(profiling runs, where the autotuner's own timings would be distorted)")
+    ap.add_argument("--msm-window-bits", type=int, default=0,
+                    help="0 = the context's choice (11-bit fixed-base tables when they fit), 8 = 8-bit windows "
+                         "without tables (a few GB on the device: profiling captures of the RS / Merkle kernels)")
     ap.add_argument("--dims", default="10,10",
                     help="LOG_ROW,LOG_COL of the blob; the default 10,10 is the benchmark workload, smaller "
                          "shapes are for profiling captures")
@@ -524,10 +530,16 @@ def main():
                                 device_id=torch.device("cuda", local))
     pkg = load_pkg()
     L = pkg.lib()
-    params = pkg.ZgEncoderParams.from_seed(LOG_ROW, LOG_COL, PARAM_SEED, device=local)
+    params = pkg.ZgEncoderParams.from_seed(LOG_ROW, LOG_COL, PARAM_SEED, device=local,
+                                           msm_window_bits=args.msm_window_bits)
     # the kernels' free choices (MSM product kind, RS tile shape), timed on a
     # synthetic blob before any measurement
-    tuning = params.autotune()
+    if args.tuning:
+        prod_kind, cols, threads = args.tuning.split(",")
+        params.set_tuning(prod_kind, int(cols), int(threads))
+        tuning = dict(params.tuning(), source="--tuning")
+    else:
+        tuning = params.autotune()
     payload = np.random.default_rng(DATA_SEED + rank).integers(0, 256, size=PAYLOAD, dtype=np.uint8)
     d_payload = torch.from_numpy(payload.copy()).cuda()
     h_payload = torch.from_numpy(payload.copy()).pin_memory()
@@ -642,7 +654,7 @@ def main():
     # batched verification of every slice of one blob (EncodedSlice::verify for
     # 3072 slices through zg_verify_slices), beside the oracle's per-slice
     # verifier on a sample
-    if world == 1 and args.verify_sample > 0:
+    if world == 1 and args.verify_sample > 0 and args.msm_window_bits != 8:  # needs the fixed-base tables
         rep = pkg.EncoderService(params).process_data(payload.tobytes(), True)
         times = []
         for k in range(2):
