@@ -68,7 +68,8 @@ class _DeviceBlob(ctypes.Structure):
 class _Tuning(ctypes.Structure):
     """zg_tuning (include/zg_encoder.h)."""
     _fields_ = [("msm_product", ctypes.c_uint32), ("ntt_cols_per_cta", ctypes.c_uint32),
-                ("ntt_threads", ctypes.c_uint32), ("msm_ms", ctypes.c_float * 3), ("ntt_ms", ctypes.c_float * 9)]
+                ("ntt_threads", ctypes.c_uint32), ("msm_ms", ctypes.c_float * 3), ("ntt_ms", ctypes.c_float * 9),
+                ("msm_wide_lines", ctypes.c_uint32)]
 
 
 MSM_PRODUCTS = ("imad", "hybrid", "fp64")  # ZG_MSM_PRODUCT_IMAD / _HYBRID / _FP64
@@ -77,7 +78,7 @@ MSM_PRODUCTS = ("imad", "hybrid", "fp64")  # ZG_MSM_PRODUCT_IMAD / _HYBRID / _FP
 def _tuning_dict(t):
     return {"msm_product": MSM_PRODUCTS[t.msm_product], "ntt_cols_per_cta": t.ntt_cols_per_cta,
             "ntt_threads": t.ntt_threads, "msm_ms": [round(x, 4) for x in t.msm_ms],
-            "ntt_ms": [round(x, 4) for x in t.ntt_ms]}
+            "ntt_ms": [round(x, 4) for x in t.ntt_ms], "msm_wide_lines": t.msm_wide_lines}
 
 
 _P = ctypes.c_void_p

@@ -172,6 +172,7 @@ int set_smem_limits() {
   ZG_CK(cudaFuncSetAttribute(k_rows_ntt, cudaFuncAttributeMaxDynamicSharedMemorySize, big));
   ZG_CK(cudaFuncSetAttribute(k_msm_chunks, cudaFuncAttributeMaxDynamicSharedMemorySize, big));
   ZG_CK(cudaFuncSetAttribute(k_fb_sort, cudaFuncAttributeMaxDynamicSharedMemorySize, big));
+  ZG_CK(cudaFuncSetAttribute(k_wd_sort, cudaFuncAttributeMaxDynamicSharedMemorySize, big));
   ZG_CK(cudaFuncSetAttribute(k_ntt4_colpass, cudaFuncAttributeMaxDynamicSharedMemorySize, big));
   ZG_CK(cudaFuncSetAttribute(k_ntt4_rowpass, cudaFuncAttributeMaxDynamicSharedMemorySize, big));
   done = true;
@@ -225,6 +226,15 @@ struct zg_ctx {
   XYZZ* fb_S = nullptr;
   XYZZ* fb_gbuf = nullptr;  // per persistent CTA task partial sums
   unsigned fb_ctas[3] = {0, 0, 0};  // resident CTAs of k_fb_accum per product kind
+  unsigned wd_ctas[3] = {0, 0, 0};  // the same for the wide-item kernels
+  // wide windows (16-bit digits over 2^15-point units) for the AMT lines whose
+  // nodes hold >= 2^15 points: quotient lines 0 .. nwq - 1 and the high line;
+  // nwl = nwq + 1 wide lines, 0 when the context has none.
+  // wtab[c][wl][WD_WINDOWS][N]; wd_offs / wd_ents = k_wd_sort's output.
+  int nwq = 0, nwl = 0;
+  G1Aff* wtab = nullptr;
+  uint32_t* wd_offs = nullptr;
+  uint32_t* wd_ents = nullptr;
   // free choices of the kernels (zg_ctx_autotune / zg_ctx_set_tuning); the
   // defaults are the fastest on the B200. tuning_gen counts changes, so the
   // request pipeline re-captures its CUDA graphs.
@@ -340,6 +350,18 @@ int alloc_blob_buffers(zg_ctx* c) {
     for (int k = 0; k < 3; ++k) {
       c->fb_ctas[k] = (unsigned)std::max(1, sms * std::max(1, per_sm[k]));
       most = std::max(most, c->fb_ctas[k]);
+    }
+    if (c->nwl) {
+      const size_t units = c->N >> WD_UNIT_LOG;
+      ZG_CK(cudaMalloc(&c->wd_offs, 3 * units * (WD_BUCKETS + 1) * sizeof(uint32_t)));
+      ZG_CK(cudaMalloc(&c->wd_ents, 3 * units * WD_UNIT_ENTS * sizeof(uint32_t)));
+      ZG_CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm[0], k_fb_accum<MulImad, true>, FB_ACC_THREADS, 0));
+      ZG_CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm[1], k_fb_accum<MulHybrid, true>, FB_ACC_THREADS, 0));
+      ZG_CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm[2], k_fb_accum<MulF64, true>, FB_ACC_THREADS, 0));
+      for (int k = 0; k < 3; ++k) {
+        c->wd_ctas[k] = (unsigned)std::max(1, sms * std::max(1, per_sm[k]));
+        most = std::max(most, c->wd_ctas[k]);
+      }
     }
     ZG_CK(cudaMalloc(&c->fb_gbuf, (size_t)most * FB_MAX_TASKS * sizeof(XYZZ)));
   }
@@ -559,22 +581,54 @@ BlobBufs ctx_bufs(zg_ctx* c) {
 // Kernel launches of one encode: 3 RS passes, leaves + tree_depth parent
 // levels, file root, MSM (sort, accumulate, combine or chunks, combine),
 // trees, serialisation, slices.
-uint64_t launches_per_encode(const zg_ctx* c) { return 3 + (uint64_t)c->tree_depth + 1 + 1 + (c->fb ? 3 : 2) + 1 + 1 + 1; }
+uint64_t launches_per_encode(const zg_ctx* c) {
+  return 3 + (uint64_t)c->tree_depth + 1 + 1 + (c->fb ? 3 : 2) + (c->nwl ? 3 : 0) + 1 + 1 + 1;
+}
 
-// the blob MSM's work items: (coset, chunk, line) over the context's tables
+// the blob MSM's chunk work items: (coset, chunk, line) over the 11-bit
+// tables, for the lines that have no wide windows (nwq .. L - 2, and the high
+// line L - 1 when the context has no wide lines)
 FbAccArgs blob_fb_args(const zg_ctx* c) {
   FbAccArgs fa;
   fa.tab = c->tab;
   fa.offs = c->fb_offs;
   fa.ents = c->fb_ents;
+  fa.ents32 = nullptr;
   fa.outT = c->fb_T;
   fa.outS = c->fb_S;
   fa.lr = c->lr;
   fa.lc = c->lc;
-  fa.lines = c->L;
+  fa.lines = c->L - c->nwl;
+  fa.l0 = c->nwq;
+  fa.Ltot = c->L;
   fa.tabN = c->N;
   return fa;
 }
+FbCombineMap blob_fb_map(const zg_ctx* c) { return FbCombineMap{c->lr, c->L - c->nwl, c->nwq, c->L, 0, 0}; }
+
+// the blob MSM's wide work items: (coset, unit block, wide line); their
+// (T, S) partials follow the chunk items' in fb_T / fb_S
+size_t blob_wd_first(const zg_ctx* c) { return (size_t)3 * c->R * (c->L - c->nwl) * FB_ACC_THREADS; }
+FbAccArgs blob_wd_args(const zg_ctx* c) {
+  FbAccArgs fa;
+  fa.tab = c->wtab;
+  fa.offs = c->wd_offs;
+  fa.ents = nullptr;
+  fa.ents32 = c->wd_ents;
+  fa.outT = c->fb_T + blob_wd_first(c);
+  fa.outS = c->fb_S + blob_wd_first(c);
+  fa.lr = c->lr;
+  fa.lc = c->lc;
+  fa.lines = c->nwl;
+  fa.l0 = 0;
+  fa.Ltot = c->nwl;
+  fa.tabN = c->N;
+  return fa;
+}
+FbCombineMap blob_wd_map(const zg_ctx* c) { return FbCombineMap{c->lr, c->nwl, 0, c->L, 1, 1}; }
+
+// one item set of a single MSM over table line `line` of `tab` (lines = 1)
+FbCombineMap single_fb_map(int lr) { return FbCombineMap{lr, 1, 0, 1, 0, 0}; }
 
 // seeded pseudo-random payload bytes (the autotuner's synthetic blob)
 __global__ void k_fill_payload(uint8_t* p, uint64_t n, uint64_t seed) {
@@ -587,12 +641,30 @@ __global__ void k_fill_payload(uint8_t* p, uint64_t n, uint64_t seed) {
   }
 }
 
-// k_fb_accum over `units` work items with product kind `kind`
-void launch_fb_accum(const zg_ctx* c, uint32_t kind, const FbAccArgs& fa, uint32_t units, cudaStream_t s) {
-  const unsigned grid = std::min<unsigned>(c->fb_ctas[kind], units);
+// k_fb_accum over `units` work items with product kind `kind` (chunk items,
+// or wide items when `wide`)
+void launch_fb_accum(const zg_ctx* c, uint32_t kind, const FbAccArgs& fa, uint32_t units, cudaStream_t s,
+                     bool wide = false) {
+  const unsigned grid = std::min<unsigned>(wide ? c->wd_ctas[kind] : c->fb_ctas[kind], units);
+  if (wide) {
+    if (kind == ZG_MSM_PRODUCT_IMAD) k_fb_accum<MulImad, true><<<grid, FB_ACC_THREADS, 0, s>>>(fa, c->fb_gbuf, units);
+    else if (kind == ZG_MSM_PRODUCT_FP64) k_fb_accum<MulF64, true><<<grid, FB_ACC_THREADS, 0, s>>>(fa, c->fb_gbuf, units);
+    else k_fb_accum<MulHybrid, true><<<grid, FB_ACC_THREADS, 0, s>>>(fa, c->fb_gbuf, units);
+    return;
+  }
   if (kind == ZG_MSM_PRODUCT_IMAD) k_fb_accum<MulImad><<<grid, FB_ACC_THREADS, 0, s>>>(fa, c->fb_gbuf, units);
   else if (kind == ZG_MSM_PRODUCT_FP64) k_fb_accum<MulF64><<<grid, FB_ACC_THREADS, 0, s>>>(fa, c->fb_gbuf, units);
   else k_fb_accum<MulHybrid><<<grid, FB_ACC_THREADS, 0, s>>>(fa, c->fb_gbuf, units);
+}
+
+// P = sum_i T_i + 8 sum_i i S_i per item: one thread per item for a blob's
+// items (fewest additions), one warp per item below 16 384 items
+// (the items' partials start at fb_T / fb_S + first)
+void launch_fb_combine(const zg_ctx* c, uint32_t units, const FbCombineMap& m, cudaStream_t s, size_t first = 0) {
+  const XYZZ* T = c->fb_T + first;
+  const XYZZ* S = c->fb_S + first;
+  if (units >= 16384) k_fb_combine<<<nblk(units, 64), 64, 0, s>>>(T, S, c->part, m, units);
+  else k_fb_combine_warp<<<nblk((size_t)units * 32, 128), 128, 0, s>>>(T, S, c->part, m, units);
 }
 
 // the three RS-extension passes with a given column tile and block size
@@ -631,10 +703,15 @@ int encode_launches(zg_ctx* c, const BlobBufs& b, size_t len, bool by_device_len
   if (c->fb) {
     k_fb_sort<<<dim3((unsigned)R, 3), 256, fb_sort_smem_bytes(lc), s>>>(b.enc, c->fb_offs, c->fb_ents, lr, lc, 1,
                                                                          N);
-    const uint32_t units = (uint32_t)(3 * R * c->L);
+    if (c->nwl)
+      k_wd_sort<<<dim3((unsigned)(N >> WD_UNIT_LOG), 3), WD_SORT_THREADS, wd_sort_smem_bytes(), s>>>(
+          b.enc, c->wd_offs, c->wd_ents, lr, lc, 1, N);
+    const uint32_t units = (uint32_t)(3 * R * (c->L - c->nwl)), wunits = (uint32_t)(3 * R * c->nwl);
     launch_fb_accum(c, c->msm_product, blob_fb_args(c), units, s);
+    if (c->nwl) launch_fb_accum(c, c->msm_product, blob_wd_args(c), wunits, s, true);
     mark(3);
-    k_fb_combine<<<nblk(units, 64), 64, 0, s>>>(c->fb_T, c->fb_S, c->part, lr, c->L, units);
+    launch_fb_combine(c, units, blob_fb_map(c), s);
+    if (c->nwl) launch_fb_combine(c, wunits, blob_wd_map(c), s, blob_wd_first(c));
   } else {
     MsmChunkArgs a;
     a.scalars = b.enc;
@@ -1233,6 +1310,17 @@ uint64_t le_u64(const uint8_t* p) {
   return v;
 }
 
+// 32 little-endian bytes below r (a canonical Fr), without conversion
+bool fr_canonical(const uint8_t* b) {
+  const uint32_t r[8] = {FrCfg::p0, FrCfg::p1, FrCfg::p2, FrCfg::p3, FrCfg::p4, FrCfg::p5, FrCfg::p6, FrCfg::p7};
+  for (int i = 7; i >= 0; --i) {
+    const uint32_t w = (uint32_t)b[4 * i] | (uint32_t)b[4 * i + 1] << 8 | (uint32_t)b[4 * i + 2] << 16 |
+                       (uint32_t)b[4 * i + 3] << 24;
+    if (w != r[i]) return w < r[i];
+  }
+  return false;
+}
+
 // one deserialized EncodedSlice (the fields the checks read)
 struct PSlice {
   const uint8_t* bytes = nullptr;
@@ -1259,10 +1347,8 @@ bool parse_slice(const uint8_t* in, size_t len, PSlice* s) {
   s->row_len = le_u64(p + 88);
   p += 96;
   if (s->row_len > left() / 32) return false;
-  for (uint64_t i = 0; i < s->row_len; ++i, p += 32) {
-    Fr x;
-    if (!field_from_le(p, &x)) return false;
-  }
+  for (uint64_t i = 0; i < s->row_len; ++i, p += 32)
+    if (!fr_canonical(p)) return false;
   if (left() < 8) return false;
   const uint64_t np = le_u64(p);
   p += 8;
@@ -1344,12 +1430,15 @@ int verify_msms(VerifyRun& v, const bool present[3], XYZZ* out) {
     fa.ents = c->fb_ents;
     fa.outT = c->fb_T;
     fa.outS = c->fb_S;
+    fa.ents32 = nullptr;
     fa.lr = c->lr;
     fa.lc = c->lc;
     fa.lines = 1;
+    fa.l0 = 0;
+    fa.Ltot = 1;
     fa.tabN = c->N;
     launch_fb_accum(c, c->msm_product, fa, R, v.s);
-    k_fb_combine<<<nblk(R, 64), 64, 0, v.s>>>(c->fb_T, c->fb_S, c->part, c->lr, 1, R);
+    launch_fb_combine(c, R, single_fb_map(c->lr), v.s);
     k_sum_points<<<1, 256, 0, v.s>>>(c->part, R, out + cs);
   }
   return check_launch();
@@ -1657,6 +1746,22 @@ int zg_ctx_create(const zg_config* cfg, zg_ctx** out) {
   }
   if (!c->tab && cudaMalloc(&c->tab, (size_t)3 * c->L * c->N * sizeof(G1Aff)) != cudaSuccess)
     return bail(fail(ZG_ERR_CUDA, "cannot allocate params"));
+  // wide windows for the lines whose AMT nodes hold >= 2^15 points (auto only;
+  // 1024 columns, so that a unit's 32 blocks are 32 chunks' item slots)
+  // and 8 GiB left over for the blob buffers and the request pipeline's slots
+  size_t free_b = 0, total_b = 0;
+  if (c->fb && wb == 0 && c->lc == 10 && c->lr >= WD_UNIT_LOG - c->lc &&
+      cudaMemGetInfo(&free_b, &total_b) == cudaSuccess) {
+    const int nwq = c->lr + c->lc - WD_UNIT_LOG;
+    const size_t bytes = (size_t)3 * (nwq + 1) * WD_WINDOWS * c->N * sizeof(G1Aff);
+    if (free_b >= bytes + (8ull << 30) && cudaMalloc(&c->wtab, bytes) == cudaSuccess) {
+      c->nwq = nwq;
+      c->nwl = nwq + 1;
+    } else {
+      cudaGetLastError();
+      c->wtab = nullptr;
+    }
+  }
   if ((rc = alloc_blob_buffers(c))) return bail(rc);
   if (cfg->params_dir && cfg->params_dir[0]) rc = load_mont_params(c, cfg->params_dir);
   else {
@@ -1668,6 +1773,9 @@ int zg_ctx_create(const zg_config* cfg, zg_ctx** out) {
   if (c->fb) {
     const uint64_t nl = (uint64_t)3 * c->L;
     k_fb_tables<<<nblk(nl * c->N, 128), 128, 0, c->stream>>>(c->tab, c->N, nl);
+    if (c->nwl)
+      k_wd_tables<<<nblk((uint64_t)3 * c->nwl * c->N, 128), 128, 0, c->stream>>>(c->wtab, c->tab, c->N, c->L, c->nwq,
+                                                                                  c->nwl);
     if (cudaStreamSynchronize(c->stream) != cudaSuccess || cudaGetLastError() != cudaSuccess)
       return bail(fail(ZG_ERR_CUDA, "fixed-base table build failed"));
   }
@@ -1687,7 +1795,8 @@ void zg_ctx_destroy(zg_ctx* c) {
   for (void* p : rp) if (p) cudaFree(p);
   if (c->h_rec) cudaFreeHost(c->h_rec);
   void* ps[] = {c->tab, c->raw, c->enc, c->T1, c->Bc, c->win, c->part, c->nodes, c->amt,
-                c->tree, c->tree_off_d, c->slices, c->file_root, c->fb_offs, c->fb_ents, c->fb_T, c->fb_S, c->fb_gbuf};
+                c->tree, c->tree_off_d, c->slices, c->file_root, c->fb_offs, c->fb_ents, c->fb_T, c->fb_S, c->fb_gbuf,
+                c->wtab, c->wd_offs, c->wd_ents};
   for (void* p : ps) if (p) cudaFree(p);
   if (c->h_in) cudaFreeHost(c->h_in);
   for (cudaEvent_t e : c->ev) if (e) cudaEventDestroy(e);
@@ -2080,6 +2189,7 @@ int zg_ctx_get_tuning(zg_ctx* c, zg_tuning* out) {
   out->msm_product = c->msm_product;
   out->ntt_cols_per_cta = c->ntt_cpb;
   out->ntt_threads = c->ntt_threads;
+  out->msm_wide_lines = (uint32_t)c->nwl;
   return ZG_OK;
 }
 
@@ -2133,13 +2243,18 @@ int zg_ctx_autotune(zg_ctx* c, zg_tuning* out) {
   };
   uint32_t best_msm = c->msm_product;
   if (c->fb) {
-    // a sample of every line's work items: the first 4 per resident CTA
-    const uint32_t all = (uint32_t)(3 * c->R * c->L);
+    // a sample of the chunk items and of the wide items: the first 4 per
+    // resident CTA of each
+    const uint32_t all = (uint32_t)(3 * c->R * (c->L - c->nwl)), wall = (uint32_t)(3 * c->R * c->nwl);
     const uint32_t sample = std::min<uint32_t>(all, 4 * std::max(c->fb_ctas[0], std::max(c->fb_ctas[1], c->fb_ctas[2])));
-    const FbAccArgs fa = blob_fb_args(c);
+    const uint32_t wsample = std::min<uint32_t>(wall, 4 * std::max(c->wd_ctas[0], std::max(c->wd_ctas[1], c->wd_ctas[2])));
+    const FbAccArgs fa = blob_fb_args(c), fw = blob_wd_args(c);
     float best = 0;
     for (uint32_t k = 0; k < 3; ++k) {
-      t.msm_ms[k] = timed([&] { launch_fb_accum(c, k, fa, sample, s); });
+      t.msm_ms[k] = timed([&] {
+        launch_fb_accum(c, k, fa, sample, s);
+        if (wsample) launch_fb_accum(c, k, fw, wsample, s, true);
+      });
       if (t.msm_ms[k] > 0 && (best == 0 || t.msm_ms[k] < best)) { best = t.msm_ms[k]; best_msm = k; }
     }
   }
@@ -2165,6 +2280,7 @@ int zg_ctx_autotune(zg_ctx* c, zg_tuning* out) {
   t.msm_product = best_msm;
   t.ntt_cols_per_cta = best_cpb;
   t.ntt_threads = best_th;
+  t.msm_wide_lines = (uint32_t)c->nwl;
   if (out) *out = t;
   return ZG_OK;
 }
@@ -2384,12 +2500,15 @@ int zg_ctx_msm(zg_ctx* c, uint32_t coset, uint32_t line, const void* d_scalars, 
   fa.ents = c->fb_ents;
   fa.outT = c->fb_T;
   fa.outS = c->fb_S;
+  fa.ents32 = nullptr;
   fa.lr = lrn;
   fa.lc = c->lc;
   fa.lines = 1;
+  fa.l0 = 0;
+  fa.Ltot = 1;
   fa.tabN = c->N;
   launch_fb_accum(c, c->msm_product, fa, nch, s);
-  k_fb_combine<<<nblk(nch, 64), 64, 0, s>>>(c->fb_T, c->fb_S, c->part, lrn, 1, nch);
+  launch_fb_combine(c, nch, single_fb_map(lrn), s);
   k_sum_points<<<1, 256, 0, s>>>(c->part, nch, c->nodes);
   k_serialize_nodes<<<1, 128, 0, s>>>(c->nodes, (uint8_t*)d_out, 1);
   c->launches += 5;

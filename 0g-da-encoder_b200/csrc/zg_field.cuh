@@ -229,6 +229,15 @@ struct Fp {
     uint32_t borrow = sub_raw(s, r, modulus());
     return borrow ? r : s;
 #else
+    return mul_host(a, b);
+#endif
+  }
+
+#ifndef __CUDA_ARCH__
+  // the host product, out of line: inlined into every host use of the
+  // extension-field and curve formulas it makes the host object huge and slow
+  // to compile, for no speed that matters on the host
+  __host__ __attribute__((noinline)) static Fp mul_host(const Fp& a, const Fp& b) {
     uint32_t t[10] = {0, 0, 0, 0, 0, 0, 0, 0, 0, 0};
     const Fp p = modulus();
     for (int i = 0; i < 8; ++i) {
@@ -258,8 +267,8 @@ struct Fp {
     Fp d;
     uint32_t borrow = sub_raw(d, r, p);
     return (t[8] == 0 && borrow) ? r : d;
-#endif
   }
+#endif
 
   // two independent products r1 = a*b, r2 = c*d with their CIOS rows
   // interleaved: the two carry chains have no data dependence, so either

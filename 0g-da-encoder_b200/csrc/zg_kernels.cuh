@@ -363,30 +363,43 @@ constexpr int FB_BUCKETS = 1 << (FB_BITS - 1);    // 1024
 constexpr int FB_ACC_THREADS = 128;
 constexpr int FB_PER_THREAD = FB_BUCKETS / FB_ACC_THREADS;  // 8 buckets per thread
 
-// window w's multiples: tab[(line * W + w) * N + p]; window 0 already holds the
-// bases. One thread per (line, point): 11 doublings per window, then one
-// batch inversion for the 23 affine conversions.
-__global__ void __launch_bounds__(128) k_fb_tables(G1Aff* tab, uint64_t N, uint64_t nlines) {
-  uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= nlines * N) return;
-  const uint64_t line = i / N, p = i % N;
-  G1Aff* col = tab + line * FB_WINDOWS * N + p;
-  XYZZ pts[FB_WINDOWS - 1];
+// Wide windows for the AMT lines whose nodes are MSMs over >= 2^15 points: a
+// node's 2^15-point sort units share 2^15 buckets of 16-bit signed digits, so
+// a point costs 16 bucket additions instead of 24 and the bucket reduction is
+// paid per unit instead of per 1024-point chunk. A unit's buckets are cut into
+// 32 blocks of FB_BUCKETS, each block one work item of k_fb_accum: with 1024
+// columns a (coset, line) still has exactly R items, item u * 32 + blk = block
+// blk of unit u, and a node's items are contiguous, so the AMT tree kernel
+// sums them like chunk results.
+constexpr int WD_BITS = 16;
+constexpr int WD_WINDOWS = 16;                         // 256 bits; the top digit of a scalar < r is < 2^14
+constexpr int WD_BUCKETS = 1 << (WD_BITS - 1);         // |digit| in 1 .. 2^15
+constexpr int WD_UNIT_LOG = 15;                        // points per sort unit
+constexpr int WD_UNIT = 1 << WD_UNIT_LOG;
+constexpr int WD_BLOCKS = WD_BUCKETS / FB_BUCKETS;     // 32 work items per unit
+constexpr uint64_t WD_UNIT_ENTS = (uint64_t)WD_UNIT * WD_WINDOWS;  // entry capacity of a unit
+static_assert(WD_BLOCKS * 1024 == WD_UNIT, "a unit's items are 32 chunks' worth (1024 columns)");
+
+// col[(w + 1) * N] = 2^(BITS (w + 1)) * col[0] for w < WIN - 1: BITS
+// doublings per window, then one batch inversion for the affine conversions.
+template <int BITS, int WIN>
+__device__ void fb_fill_windows(G1Aff* col, uint64_t N) {
+  XYZZ pts[WIN - 1];
   XYZZ acc = XYZZ::from_affine(col[0]);
-  for (int w = 1; w < FB_WINDOWS; ++w) {
+  for (int w = 1; w < WIN; ++w) {
 #pragma unroll 1
-    for (int k = 0; k < FB_BITS; ++k) acc = acc.dbl();
+    for (int k = 0; k < BITS; ++k) acc = acc.dbl();
     pts[w - 1] = acc;
   }
   // batch inversion of the ZZZ coordinates (bases are never infinity)
-  Fq pre[FB_WINDOWS - 1];
+  Fq pre[WIN - 1];
   Fq run = Fq::one();
-  for (int w = 0; w < FB_WINDOWS - 1; ++w) {
+  for (int w = 0; w < WIN - 1; ++w) {
     pre[w] = run;
     run = MulHybrid::mul(run, pts[w].ZZZ);
   }
   Fq inv = run.inverse();
-  for (int w = FB_WINDOWS - 2; w >= 0; --w) {
+  for (int w = WIN - 2; w >= 0; --w) {
     Fq izzz = MulHybrid::mul(inv, pre[w]);
     inv = MulHybrid::mul(inv, pts[w].ZZZ);
     Fq izz = MulHybrid::mul(MulHybrid::mul(pts[w].ZZ, pts[w].ZZ), MulHybrid::mul(izzz, izzz));
@@ -395,6 +408,30 @@ __global__ void __launch_bounds__(128) k_fb_tables(G1Aff* tab, uint64_t N, uint6
     a.y = MulHybrid::mul(pts[w].Y, izzz);
     col[(uint64_t)(w + 1) * N] = a;
   }
+}
+
+// window w's multiples: tab[(line * W + w) * N + p]; window 0 already holds the
+// bases. One thread per (line, point).
+__global__ void __launch_bounds__(128) k_fb_tables(G1Aff* tab, uint64_t N, uint64_t nlines) {
+  uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= nlines * N) return;
+  const uint64_t line = i / N, p = i % N;
+  fb_fill_windows<FB_BITS, FB_WINDOWS>(tab + line * FB_WINDOWS * N + p, N);
+}
+
+// Wide-window tables of the wide lines: wtab[((cs * nwl + wl) * WD_WINDOWS + w) * N + p]
+// = 2^(16 w) P with P = point p of AMT line (wl < nwq ? wl : L - 1) of coset
+// cs, read from window 0 of the 11-bit table tab[cs][line][FB_WINDOWS][N].
+__global__ void __launch_bounds__(128) k_wd_tables(G1Aff* wtab, const G1Aff* __restrict__ tab, uint64_t N, int L,
+                                                   int nwq, int nwl) {
+  uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= 3ull * nwl * N) return;
+  const uint64_t p = i % N, cl = i / N;  // cl = cs * nwl + wl
+  const int wl = (int)(cl % nwl), cs = (int)(cl / nwl);
+  const int line = wl < nwq ? wl : L - 1;
+  G1Aff* col = wtab + cl * WD_WINDOWS * N + p;
+  col[0] = tab[((uint64_t)cs * L + line) * FB_WINDOWS * N + p];
+  fb_fill_windows<WD_BITS, WD_WINDOWS>(col, N);
 }
 
 // signed 11-bit digit w of a scalar given as 8 little-endian u32 limbs
@@ -489,30 +526,125 @@ __global__ void __launch_bounds__(256) k_fb_sort(const uint8_t* __restrict__ sca
   for (uint32_t e = threadIdx.x; e < total; e += blockDim.x) dst[e] = lst[e];
 }
 
+constexpr int WD_SORT_THREADS = 1024;
+inline size_t wd_sort_smem_bytes() { return (size_t)(WD_BUCKETS + 1 + 32) * sizeof(uint32_t); }
+
+// Per wide sort unit (2^15 consecutive points of a coset, i.e. chunks
+// 32 u .. 32 u + 31 of 1024 columns): counting sort of the (point, window)
+// pairs by |digit| of the signed 16-bit digits.
+//   offs[cs][u][k] .. offs[cs][u][k + 1] = entries of bucket k (|digit| = k + 1)
+//   ents[cs][u][e] = p | w << 15 | sign << 31, p the point within the unit
+// Point p of unit u is chunk b = (u << 5) + (p >> 10), element t = p & 1023,
+// read like k_fb_sort reads it. Pass 1 counts, a block scan turns the counts
+// into fill pointers, pass 2 scatters (the scalars are read twice).
+__device__ __forceinline__ uint32_t wd_window_bits(const uint32_t* s, int w) {
+  return (s[w >> 1] >> ((w & 1) << 4)) & 0xffffu;
+}
+
+__global__ void __launch_bounds__(WD_SORT_THREADS) k_wd_sort(const uint8_t* __restrict__ scalars,
+                                                             uint32_t* __restrict__ offs, uint32_t* __restrict__ ents,
+                                                             int lr, int lc, int bitrev_rows,
+                                                             uint64_t scalar_coset_stride) {
+  extern __shared__ __align__(16) uint32_t wcnt[];  // [WD_BUCKETS + 1], then [32] warp sums
+  uint32_t* wsum = wcnt + WD_BUCKETS + 1;
+  const uint32_t unit = blockIdx.x, coset = blockIdx.y, nunits = gridDim.x;
+  const uint32_t C = 1u << lc;
+  const uint8_t* src = scalars + scalar_coset_stride * coset * 32;
+  uint32_t* o = offs + ((size_t)coset * nunits + unit) * (WD_BUCKETS + 1);
+  uint32_t* e = ents + ((size_t)coset * nunits + unit) * WD_UNIT_ENTS;
+  for (int k = threadIdx.x; k <= WD_BUCKETS; k += blockDim.x) wcnt[k] = 0;
+  __syncthreads();
+  for (int pass = 0; pass < 2; ++pass) {
+    for (uint32_t p = threadIdx.x; p < (uint32_t)WD_UNIT; p += blockDim.x) {
+      const uint32_t gp = (unit << WD_UNIT_LOG) + p;
+      const uint32_t b = gp >> lc, t = gp & (C - 1);
+      const uint32_t row = bitrev_rows ? brev_bits(b, lr) : b;
+      const uint32_t col = bitrev_rows ? brev_bits(t, lc) : t;
+      const uint4* q = reinterpret_cast<const uint4*>(src + ((uint64_t)row * C + col) * 32);
+      const uint4 x = q[0], y = q[1];
+      const uint32_t s[8] = {x.x, x.y, x.z, x.w, y.x, y.y, y.z, y.w};
+      uint32_t carry = 0;
+#pragma unroll
+      for (int w = 0; w < WD_WINDOWS; ++w) {
+        const uint32_t v = wd_window_bits(s, w) + carry;
+        uint32_t mag, neg;
+        if (v >= (uint32_t)WD_BUCKETS) { mag = (1u << WD_BITS) - v; neg = 1; carry = 1; }
+        else { mag = v; neg = 0; carry = 0; }
+        if (mag) {
+          const uint32_t pos = atomicAdd(&wcnt[mag - 1], 1u);
+          if (pass) e[pos] = p | (uint32_t)w << WD_UNIT_LOG | neg << 31;
+        }
+      }
+    }
+    __syncthreads();
+    if (pass == 0) {
+      // exclusive scan of the 2^15 counts: 32 per thread, warp scans, warp sums
+      const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+      const int k0 = threadIdx.x * (WD_BUCKETS / WD_SORT_THREADS);
+      uint32_t sum = 0;
+      for (int i = 0; i < WD_BUCKETS / WD_SORT_THREADS; ++i) sum += wcnt[k0 + i];
+      uint32_t incl = sum;
+      for (int d = 1; d < 32; d <<= 1) {
+        const uint32_t v = __shfl_up_sync(0xffffffffu, incl, d);
+        if (lane >= d) incl += v;
+      }
+      if (lane == 31) wsum[warp] = incl;
+      __syncthreads();
+      if (warp == 0) {
+        const uint32_t ws = wsum[lane];
+        uint32_t wi = ws;
+        for (int d = 1; d < 32; d <<= 1) {
+          const uint32_t v = __shfl_up_sync(0xffffffffu, wi, d);
+          if (lane >= d) wi += v;
+        }
+        wsum[lane] = wi - ws;
+      }
+      __syncthreads();
+      uint32_t acc = wsum[warp] + incl - sum;
+      for (int i = 0; i < WD_BUCKETS / WD_SORT_THREADS; ++i) {
+        const uint32_t v = wcnt[k0 + i];
+        wcnt[k0 + i] = acc;
+        o[k0 + i] = acc;
+        acc += v;
+      }
+      if (threadIdx.x == blockDim.x - 1) o[WD_BUCKETS] = acc;
+      __syncthreads();
+    }
+  }
+}
+
 struct FbAccArgs {
-  const G1Aff* tab;     // [cosets][lines][W][tabN]
-  const uint32_t* offs;
-  const uint16_t* ents;
-  XYZZ* outT;           // [cosets * nchunks * lines][FB_ACC_THREADS]
-  XYZZ* outS;
-  int lr, lc, lines;    // 2^lr chunks of 2^lc points per coset
-  uint64_t tabN;        // points per window table (the param line length)
+  const G1Aff* tab = nullptr;      // [cosets][Ltot][W][tabN], W = FB_WINDOWS (WD_WINDOWS for wide items)
+  const uint32_t* offs = nullptr;
+  const uint16_t* ents = nullptr;    // chunk items
+  const uint32_t* ents32 = nullptr;  // wide items (k_wd_sort's lists)
+  XYZZ* outT = nullptr;            // [cosets * nchunks * lines][FB_ACC_THREADS]
+  XYZZ* outS = nullptr;
+  int lr = 0, lc = 0, lines = 1;   // 2^lr items of each of `lines` lines per coset
+  int l0 = 0, Ltot = 1;            // item line l reads table line l0 + l of Ltot per coset
+  uint64_t tabN = 0;               // points per window table (the param line length)
 };
 
 // Persistent CTAs over the (chunk, line) work items. Per item:
-//  1. every bucket is cut into tasks of at most FB_TASK entries (the top
+//  1. every bucket is cut into tasks of at most tsz entries (the top
 //     window's digits are tiny, so buckets 1 and 2 hold ~10x the average);
+//     tsz = FB_TASK unless the item holds more than (FB_MAX_TASKS -
+//     FB_BUCKETS) * FB_TASK entries (wide items of skewed scalars), so an
+//     item never has more than FB_MAX_TASKS tasks;
 //  2. tasks are counting-sorted by size and round r gives thread i the task at
 //     sorted position 128 r + i: the 32 lanes of a warp run tasks of nearly
 //     equal length;
 //  3. task partial sums go to this CTA's scratch (gpart, L2-resident);
 //  4. thread i merges the partials of buckets 8i+1 .. 8i+8 and folds them
 //     into running sums S_i = sum B_k, T_i = sum (k - 8i) B_k.
+// WIDE items are 1024-bucket blocks of a wide sort unit (k_wd_sort): item g of
+// a coset is block g & 31 of unit g >> 5, its buckets' entries index the
+// unit's 2^15 points and 16 windows of the wide table.
 constexpr int FB_TASK = 32;
 constexpr int FB_MAX_TASKS = FB_BUCKETS + FB_WINDOWS * 1024 / FB_TASK;  // chunk <= 1024 points
 // M is the product kind of the point additions (MulImad / MulHybrid / MulF64,
 // chosen by the context's tuning; identical results).
-template <class M>
+template <class M, bool WIDE = false>
 __global__ void __launch_bounds__(FB_ACC_THREADS, 4) k_fb_accum(FbAccArgs a, XYZZ* __restrict__ gpart_all,
                                                                 uint32_t units) {
   __shared__ uint32_t soffs[FB_BUCKETS + 1];
@@ -526,13 +658,28 @@ __global__ void __launch_bounds__(FB_ACC_THREADS, 4) k_fb_accum(FbAccArgs a, XYZ
   for (uint32_t u = blockIdx.x; u < units; u += gridDim.x) {
     const uint32_t l = u % a.lines, g = u / a.lines;
     const uint32_t coset = g / nch, b = g % nch;
-    const uint32_t* offs = a.offs + (size_t)g * (FB_BUCKETS + 1);
-    const uint16_t* ents = a.ents + (size_t)g * FB_WINDOWS * (1u << a.lc);
-    const G1Aff* tabl = a.tab + ((uint64_t)coset * a.lines + l) * FB_WINDOWS * N + ((uint64_t)b << a.lc);
+    const uint32_t* offs;
+    const uint16_t* ents = nullptr;
+    const uint32_t* ents32 = nullptr;
+    const G1Aff* tabl;
+    if constexpr (WIDE) {
+      const uint32_t unit = b / WD_BLOCKS, blk = b % WD_BLOCKS;
+      const size_t cu = (size_t)coset * (nch / WD_BLOCKS) + unit;
+      offs = a.offs + cu * (WD_BUCKETS + 1) + (size_t)blk * FB_BUCKETS;
+      ents32 = a.ents32 + cu * WD_UNIT_ENTS;
+      tabl = a.tab + ((uint64_t)coset * a.Ltot + a.l0 + l) * WD_WINDOWS * N + ((uint64_t)unit << WD_UNIT_LOG);
+    } else {
+      offs = a.offs + (size_t)g * (FB_BUCKETS + 1);
+      ents = a.ents + (size_t)g * FB_WINDOWS * (1u << a.lc);
+      tabl = a.tab + ((uint64_t)coset * a.Ltot + a.l0 + l) * FB_WINDOWS * N + ((uint64_t)b << a.lc);
+    }
     __syncthreads();  // the previous item is finished with the shared arrays and gpart
     for (int k = threadIdx.x; k <= FB_BUCKETS; k += blockDim.x) soffs[k] = offs[k];
     for (int k = threadIdx.x; k <= FB_TASK; k += blockDim.x) bins[k] = 0;
     __syncthreads();
+    const uint32_t nent = soffs[FB_BUCKETS] - soffs[0];
+    const uint32_t cap = (uint32_t)(FB_MAX_TASKS - FB_BUCKETS);
+    const uint32_t tsz = max((uint32_t)FB_TASK, (nent + cap - 1) / cap);
     // tasks per bucket, exclusive scan -> tstart (bucket k = 0-based index)
     if (threadIdx.x < 32) {
       // warp-level scan over 1024 buckets, 32 per lane
@@ -542,7 +689,7 @@ __global__ void __launch_bounds__(FB_ACC_THREADS, 4) k_fb_accum(FbAccArgs a, XYZ
       for (int i = 0; i < 32; ++i) {
         const int k = lane * 32 + i;
         const uint32_t c = soffs[k + 1] - soffs[k];
-        loc[i] = (c + FB_TASK - 1) / FB_TASK;
+        loc[i] = (c + tsz - 1) / tsz;
         sum += loc[i];
       }
       uint32_t incl = sum;
@@ -559,14 +706,15 @@ __global__ void __launch_bounds__(FB_ACC_THREADS, 4) k_fb_accum(FbAccArgs a, XYZ
     }
     __syncthreads();
     const uint32_t ntasks = tstart[FB_BUCKETS];
-    // size of task j of bucket k: FB_TASK except the bucket's last task
+    // size of task j of bucket k: tsz except the bucket's last task; bin
+    // FB_TASK - size * FB_TASK / tsz (the size itself when tsz = FB_TASK)
     for (int k = threadIdx.x; k < FB_BUCKETS; k += blockDim.x) {
       const uint32_t c = soffs[k + 1] - soffs[k];
       for (uint32_t t = tstart[k]; t < tstart[k + 1]; ++t) {
         tbucket[t] = (uint16_t)k;
         const uint32_t j = t - tstart[k];
-        const uint32_t sz = min((uint32_t)FB_TASK, c - j * FB_TASK);
-        atomicAdd(&bins[FB_TASK - sz], 1u);
+        const uint32_t sz = min(tsz, c - j * tsz);
+        atomicAdd(&bins[FB_TASK - sz * FB_TASK / tsz], 1u);
       }
     }
     __syncthreads();
@@ -579,20 +727,29 @@ __global__ void __launch_bounds__(FB_ACC_THREADS, 4) k_fb_accum(FbAccArgs a, XYZ
       const uint32_t k = tbucket[t];
       const uint32_t c = soffs[k + 1] - soffs[k];
       const uint32_t j = t - tstart[k];
-      const uint32_t sz = min((uint32_t)FB_TASK, c - j * FB_TASK);
-      order[atomicAdd(&bins[FB_TASK - sz], 1u)] = (uint16_t)t;
+      const uint32_t sz = min(tsz, c - j * tsz);
+      order[atomicAdd(&bins[FB_TASK - sz * FB_TASK / tsz], 1u)] = (uint16_t)t;
     }
     __syncthreads();
     for (uint32_t r = threadIdx.x; r < ntasks; r += blockDim.x) {
       const uint32_t t = order[r];
       const uint32_t k = tbucket[t];
-      const uint32_t e0 = soffs[k] + (t - tstart[k]) * FB_TASK;
-      const uint32_t e1 = min(e0 + FB_TASK, soffs[k + 1]);
+      const uint32_t e0 = soffs[k] + (t - tstart[k]) * tsz;
+      const uint32_t e1 = min(e0 + tsz, soffs[k + 1]);
       XYZZ B = XYZZ::inf();
       for (uint32_t e = e0; e < e1; ++e) {
-        const uint32_t v = ents[e];
-        G1Aff p = load_aff(tabl + (uint64_t)((v >> 10) & 31) * N + (v & 0x3ff));
-        if (v & 0x8000) p.y = -p.y;
+        G1Aff p;
+        bool neg;
+        if constexpr (WIDE) {
+          const uint32_t v = ents32[e];
+          p = load_aff(tabl + (uint64_t)((v >> WD_UNIT_LOG) & (WD_WINDOWS - 1)) * N + (v & (WD_UNIT - 1)));
+          neg = v >> 31;
+        } else {
+          const uint32_t v = ents[e];
+          p = load_aff(tabl + (uint64_t)((v >> 10) & 31) * N + (v & 0x3ff));
+          neg = v & 0x8000;
+        }
+        if (neg) p.y = -p.y;
         B.template add_affine<M>(p.x, p.y);
       }
       store_xyzz(gpart + t, B);
@@ -609,15 +766,41 @@ __global__ void __launch_bounds__(FB_ACC_THREADS, 4) k_fb_accum(FbAccArgs a, XYZ
   }
 }
 
-// Per (chunk, line): P = sum_i T_i + 8 * sum_i i S_i; written to
-// part[(coset * lines + l) * nchunks + b] for the AMT trees.
-__global__ void __launch_bounds__(64) k_fb_combine(const XYZZ* __restrict__ T, const XYZZ* __restrict__ S, XYZZ* __restrict__ part,
-                             int lr, int lines, uint32_t count) {
+// Where a launch's items go: item u of line l = u % lines (g = u / lines,
+// coset g >> lr, b = g & (2^lr - 1)) is written to part[(coset * L + line) *
+// 2^lr + b], line = L - 1 for the launch's last line when hi_last, else l0 + l.
+// Wide items (block blk = b & 31 of a wide unit) add 1024 blk * sum_k B_k:
+// their buckets hold digits 1024 blk + k + 1.
+struct FbCombineMap {
+  int lr, lines, l0, L, hi_last, wide;
+};
+
+__device__ __forceinline__ size_t fb_part_index(const FbCombineMap& m, uint32_t u) {
+  const uint32_t l = u % m.lines, g = u / m.lines;
+  const uint32_t nch = 1u << m.lr;
+  const uint32_t line = (m.hi_last && l == (uint32_t)m.lines - 1) ? (uint32_t)m.L - 1 : (uint32_t)m.l0 + l;
+  return ((size_t)(g / nch) * m.L + line) * nch + (g % nch);
+}
+
+// (1024 blk) * P for blk < 32
+__device__ XYZZ fb_block_term(const XYZZ& P, uint32_t blk) {
+  XYZZ r = XYZZ::inf();
+#pragma unroll 1
+  for (int bit = 4; bit >= 0; --bit) {
+    r = r.dbl();
+    if ((blk >> bit) & 1) r.add(P);
+  }
+#pragma unroll 1
+  for (int k = 0; k < 10; ++k) r = r.dbl();
+  return r;
+}
+
+// Per item: P = sum_i T_i + 8 * sum_i i S_i (+ the wide block term); written
+// to part for the AMT trees.
+__global__ void __launch_bounds__(64) k_fb_combine(const XYZZ* __restrict__ T, const XYZZ* __restrict__ S,
+                                                   XYZZ* __restrict__ part, FbCombineMap m, uint32_t count) {
   const uint32_t u = blockIdx.x * blockDim.x + threadIdx.x;
   if (u >= count) return;
-  const uint32_t l = u % lines, g = u / lines;
-  const uint32_t nch = 1u << lr;
-  const uint32_t coset = g / nch, b = g % nch;
   const XYZZ* t = T + (size_t)u * FB_ACC_THREADS;
   const XYZZ* s = S + (size_t)u * FB_ACC_THREADS;
   XYZZ tot = XYZZ::inf(), run = XYZZ::inf(), wsum = XYZZ::inf();
@@ -629,7 +812,73 @@ __global__ void __launch_bounds__(64) k_fb_combine(const XYZZ* __restrict__ T, c
 #pragma unroll 1
   for (int k = 0; k < 3; ++k) wsum = wsum.dbl();  // x FB_PER_THREAD = 8
   tot.add(wsum);
-  store_xyzz(part + ((size_t)coset * lines + l) * nch + b, tot);
+  if (m.wide) {
+    const uint32_t blk = (u / m.lines) % WD_BLOCKS;
+    if (blk) {
+      run.add(load_xyzz(s));  // sum of all the item's buckets
+      tot.add(fb_block_term(run, blk));
+    }
+  }
+  store_xyzz(part + fb_part_index(m, u), tot);
+}
+
+__device__ __forceinline__ XYZZ shfl_xor_xyzz(const XYZZ& p, int m) {
+  XYZZ r;
+#pragma unroll
+  for (int i = 0; i < 8; ++i) {
+    r.X.v[i] = __shfl_xor_sync(0xffffffffu, p.X.v[i], m);
+    r.Y.v[i] = __shfl_xor_sync(0xffffffffu, p.Y.v[i], m);
+    r.ZZ.v[i] = __shfl_xor_sync(0xffffffffu, p.ZZ.v[i], m);
+    r.ZZZ.v[i] = __shfl_xor_sync(0xffffffffu, p.ZZZ.v[i], m);
+  }
+  return r;
+}
+
+// k_fb_combine with one warp per item, for launches with few items (the
+// single MSMs of zg_ctx_msm and of slice verification: 1024 items leave
+// k_fb_combine's one thread per item on a handful of SMs). Lane l folds
+// partials 4l .. 4l+3 into t_l, s_l and w_l = sum_k k S_{4l+k}; then
+// sum_i i S_i = 4 sum_l l s_l + sum_l w_l, sum_l l s_l being the sum over
+// lanes l >= 1 of the suffix sums U_l = sum_{m >= l} s_m (a warp scan). About
+// three times the additions of k_fb_combine, so blob encodes keep that one.
+__global__ void __launch_bounds__(128) k_fb_combine_warp(const XYZZ* __restrict__ T, const XYZZ* __restrict__ S,
+                                                         XYZZ* __restrict__ part, FbCombineMap m, uint32_t count) {
+  static_assert(FB_ACC_THREADS == 128, "four partials per lane");
+  const uint32_t u = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const int lane = threadIdx.x & 31;
+  if (u >= count) return;  // uniform per warp
+  const XYZZ* t = T + (size_t)u * FB_ACC_THREADS + 4 * lane;
+  const XYZZ* s = S + (size_t)u * FB_ACC_THREADS + 4 * lane;
+  XYZZ tl = load_xyzz(t);
+  for (int k = 1; k < 4; ++k) tl.add(load_xyzz(t + k));
+  XYZZ run = load_xyzz(s + 3), w = run;
+  for (int k = 2; k >= 1; --k) {
+    run.add(load_xyzz(s + k));
+    w.add(run);
+  }
+  run.add(load_xyzz(s));
+  XYZZ U = run;
+  for (int d = 1; d < 32; d <<= 1) {
+    const XYZZ v = shfl_down_xyzz(U, d);
+    if (lane + d < 32) U.add(v);
+  }
+  XYZZ a = lane >= 1 ? U : XYZZ::inf();
+  for (int mk = 16; mk >= 1; mk >>= 1) {
+    tl.add(shfl_xor_xyzz(tl, mk));
+    w.add(shfl_xor_xyzz(w, mk));
+    a.add(shfl_xor_xyzz(a, mk));
+  }
+  if (lane == 0) {
+    a = a.dbl().dbl();        // 4 sum_l l s_l
+    a.add(w);                 // sum_i i S_i
+    a = a.dbl().dbl().dbl();  // x FB_PER_THREAD = 8
+    tl.add(a);
+    if (m.wide) {
+      const uint32_t blk = (u / m.lines) % WD_BLOCKS;
+      if (blk) tl.add(fb_block_term(U, blk));  // U at lane 0 = sum of all the item's buckets
+    }
+    store_xyzz(part + fb_part_index(m, u), tl);
+  }
 }
 
 // out = sum of the n points of `in` (one CTA of 256 threads)

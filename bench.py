@@ -103,10 +103,11 @@ def parse():
     ap.add_argument("--cpu-sample", type=int, default=0, help="chunk groups in the CPU sample (0 = auto)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--batch-blobs", type=int, default=8, help="blobs in the batched-uneven sample")
-    ap.add_argument("--serve-rate", type=float, default=2.0, help="Poisson arrival rate of the serving sample (1/s)")
-    ap.add_argument("--serve-requests", type=int, default=16, help="requests in the serving sample (0 = skip)")
-    ap.add_argument("--serve-plain", action="store_true",
-                    help="also serve the same arrivals through the blocking per-blob path")
+    ap.add_argument("--serve-rate", default="2,8",
+                    help="Poisson arrival rates of the serving sample (1/s, comma-separated sweep)")
+    ap.add_argument("--serve-requests", type=int, default=16, help="requests per serving sample (0 = skip)")
+    ap.add_argument("--no-serve-plain", action="store_true",
+                    help="skip serving the same arrivals through the blocking per-blob path")
     ap.add_argument("--verify-sample", type=int, default=4,
                     help="slices of the CPU verification sample (0 = skip the verification measurement)")
     ap.add_argument("--micro", action="store_true",
@@ -645,11 +646,13 @@ def main():
         rows = [rows_reply.encoded_data[i * (32 << LOG_COL):(i + 1) * (32 << LOG_COL)] for i in range(3 * R)]
         recs = recovery_inputs(rows, [11, 12, 13])
         full = payload.tobytes()
-        extra["serving"] = [serving_run(pkg, params, pipe, h_ptr, full, recs, args.serve_rate,
-                                        args.serve_requests, 5)]
-        if args.serve_plain:
-            extra["serving"].append(serving_run(pkg, params, pipe, h_ptr, full, recs, args.serve_rate,
-                                                args.serve_requests, 5, plain=True))
+        extra["serving"] = []
+        for rate in [float(x) for x in str(args.serve_rate).split(",") if x]:
+            extra["serving"].append(serving_run(pkg, params, pipe, h_ptr, full, recs, rate,
+                                                args.serve_requests, 5))
+            if not args.no_serve_plain:
+                extra["serving"].append(serving_run(pkg, params, pipe, h_ptr, full, recs, rate,
+                                                    args.serve_requests, 5, plain=True))
 
     # batched verification of every slice of one blob (EncodedSlice::verify for
     # 3072 slices through zg_verify_slices), beside the oracle's per-slice

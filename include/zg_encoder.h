@@ -47,8 +47,11 @@ typedef struct zg_config {
   uint64_t tau_seed;       /* params from a seeded tau when params_dir is NULL */
   const char* params_dir;  /* else: amt-prove-coset{0,1,2}-mont-*-{LR:02}-{LR+LC:02}.bin */
   int device;              /* CUDA device ordinal */
-  uint32_t msm_window_bits;/* 0 = auto (11-bit fixed-base windows when the window
-                              tables fit in HBM, else 8-bit), 11, or 8 */
+  uint32_t msm_window_bits;/* 0 = auto: 11-bit fixed-base windows when the window
+                              tables fit in HBM (else 8-bit), and with 1024
+                              columns 16-bit fixed-base windows for the AMT
+                              lines whose nodes hold >= 2^15 points when those
+                              tables fit too; 11 = 11-bit tables only; 8 */
 } zg_config;
 
 /* Builds the device-resident encoder params (3 cosets x (LR + 2) G1 lines).
@@ -120,6 +123,7 @@ typedef struct zg_tuning {
   uint32_t ntt_threads;
   float msm_ms[3];
   float ntt_ms[9];
+  uint32_t msm_wide_lines; /* read-only: AMT lines on 16-bit windows (0 = none) */
 } zg_tuning;
 int zg_ctx_autotune(zg_ctx* ctx, zg_tuning* out);
 int zg_ctx_get_tuning(zg_ctx* ctx, zg_tuning* out);

@@ -316,6 +316,32 @@ def test_device_encode_then_host_encode_are_ordered(gpu_pkg, oracle):
     params.close()
 
 
+@pytest.mark.parametrize("log_row", [5, 6])
+def test_encode_wide_windows_match_oracle(gpu_pkg, oracle, log_row):
+    """With 1024 columns the AMT lines whose nodes hold >= 2^15 points run on
+    16-bit fixed-base windows over 2^15-point units (32 rows: the high line;
+    64 rows: also quotient line 0). Both a random payload and a constant one
+    (every data scalar equal: whole units in one bucket per window, the
+    adaptive task size of the bucket kernel) give the oracle's bytes, and the
+    11-bit-only context gives the same reply."""
+    seed = 41
+    params = gpu_pkg.ZgEncoderParams.from_seed(log_row, 10, seed)
+    narrow = gpu_pkg.ZgEncoderParams.from_seed(log_row, 10, seed, msm_window_bits=11)
+    assert params.tuning()["msm_wide_lines"] == log_row - 4
+    assert narrow.tuning()["msm_wide_lines"] == 0
+    op = oracle.params(log_row, 10, seed)
+    d = params.dims
+    rng = np.random.default_rng(log_row)
+    for payload in (rng.integers(0, 256, size=d.max_raw_data_size, dtype=np.uint8).tobytes(),
+                    b"\xff" * d.max_raw_data_size):
+        reply = _check_against_oracle(gpu_pkg, oracle, params, op, payload)
+        other = gpu_pkg.EncoderService(narrow).process_data(payload, False)
+        assert other.erasure_commitment == reply.erasure_commitment
+        assert list(other.encoded_slice) == list(reply.encoded_slice)
+    narrow.close()
+    params.close()
+
+
 def test_encode_zero_blob_is_infinity(gpu_pkg, oracle):
     """An empty payload encodes to the all-zero blob: every commitment and
     proof is the point at infinity (ark flag bit 6)."""

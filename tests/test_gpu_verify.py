@@ -147,3 +147,30 @@ def test_production_blob_verifies(prod, gpu_pkg, oracle):
     assert rc == zgo.V_AMT_INCORRECT_PROOF and d[0] == zgo.P_INCONSISTENT
     assert codes[1500] == rc and det[1500] == d
     assert codes[:1500] == [0] * 1500 and codes[1501:] == [0] * 1571
+
+
+def test_mont_param_files(gpu_pkg, oracle, tmp_path):
+    """ZgEncoderParams::from_dir_mont (crates/amt/src/blob/encode.rs:114-132):
+    params read from the reference's mont files (G1 lines and the G2
+    vanishing points / high_g2 the verifier needs) encode and verify exactly
+    as the seeded context does."""
+    lr, lc, seed = 4, 6, 57
+    op = oracle.params(lr, lc, seed)
+    for c in range(3):
+        # the reference's file names: amt-prove-coset{c}-mont-<hash>-{LR:02}-{LR+LC:02}.bin
+        (tmp_path / f"amt-prove-coset{c}-mont-5DWgDV-{lr:02d}-{lr + lc:02d}.bin").write_bytes(op.mont(c))
+    params = gpu_pkg.ZgEncoderParams.from_dir_mont(str(tmp_path), lr, lc)
+    seeded = gpu_pkg.ZgEncoderParams.from_seed(lr, lc, seed)
+    for c in range(3):
+        for line in range(lr + 2):
+            assert params.param_line(c, line) == seeded.param_line(c, line)
+    payload = np.random.default_rng(4).integers(0, 256, size=params.dims.max_raw_data_size,
+                                                dtype=np.uint8).tobytes()
+    reply = gpu_pkg.EncoderService(params).process_data(payload, True)
+    ob = oracle.encode(op, payload)
+    assert reply.erasure_commitment == ob.commitment() and reply.storage_root == ob.file_root()
+    codes = _check_same(gpu_pkg, oracle, params, op, reply.encoded_slice, reply.erasure_commitment,
+                        reply.storage_root)
+    assert codes == [0] * len(reply.encoded_slice)
+    params.close()
+    seeded.close()
