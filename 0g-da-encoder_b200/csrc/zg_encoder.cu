@@ -172,7 +172,11 @@ int set_smem_limits() {
   ZG_CK(cudaFuncSetAttribute(k_rows_ntt, cudaFuncAttributeMaxDynamicSharedMemorySize, big));
   ZG_CK(cudaFuncSetAttribute(k_msm_chunks, cudaFuncAttributeMaxDynamicSharedMemorySize, big));
   ZG_CK(cudaFuncSetAttribute(k_fb_sort, cudaFuncAttributeMaxDynamicSharedMemorySize, big));
-  ZG_CK(cudaFuncSetAttribute(k_wd_sort, cudaFuncAttributeMaxDynamicSharedMemorySize, big));
+  ZG_CK(cudaFuncSetAttribute(k_wd_sort<15>, cudaFuncAttributeMaxDynamicSharedMemorySize, big));
+  ZG_CK(cudaFuncSetAttribute(k_wd_sort<14>, cudaFuncAttributeMaxDynamicSharedMemorySize, big));
+  ZG_CK(cudaFuncSetAttribute(k_wd_sort<13>, cudaFuncAttributeMaxDynamicSharedMemorySize, big));
+  ZG_CK(cudaFuncSetAttribute(k_wd_sort<12>, cudaFuncAttributeMaxDynamicSharedMemorySize, big));
+  ZG_CK(cudaFuncSetAttribute(k_wd_sort<11>, cudaFuncAttributeMaxDynamicSharedMemorySize, big));
   ZG_CK(cudaFuncSetAttribute(k_ntt4_colpass, cudaFuncAttributeMaxDynamicSharedMemorySize, big));
   ZG_CK(cudaFuncSetAttribute(k_ntt4_rowpass, cudaFuncAttributeMaxDynamicSharedMemorySize, big));
   done = true;
@@ -225,16 +229,26 @@ struct zg_ctx {
   XYZZ* fb_T = nullptr;
   XYZZ* fb_S = nullptr;
   XYZZ* fb_gbuf = nullptr;  // per persistent CTA task partial sums
+  uint32_t* fb_next = nullptr;  // k_fb_accum's item counter
   unsigned fb_ctas[3] = {0, 0, 0};  // resident CTAs of k_fb_accum per product kind
-  unsigned wd_ctas[3] = {0, 0, 0};  // the same for the wide-item kernels
-  // wide windows (16-bit digits over 2^15-point units) for the AMT lines whose
-  // nodes hold >= 2^15 points: quotient lines 0 .. nwq - 1 and the high line;
-  // nwl = nwq + 1 wide lines, 0 when the context has none.
-  // wtab[c][wl][WD_WINDOWS][N]; wd_offs / wd_ents = k_wd_sort's output.
-  int nwq = 0, nwl = 0;
-  G1Aff* wtab = nullptr;
-  uint32_t* wd_offs = nullptr;
-  uint32_t* wd_ents = nullptr;
+  // Wide-window classes (k_wd_sort): class k sorts units of 2^ulog points
+  // into 2^ulog buckets of (ulog + 1)-bit digits, for AMT lines l0 .. l0 +
+  // nl - 1 (the last one the high line L - 1 when hi_last); tab[c][wl][W][N]
+  // holds their window multiples, offs / ents the sort output. The 11-bit
+  // chunk items cover the other lines, n_l0 .. n_l0 + n_lines - 1.
+  struct WdClass {
+    int ulog = 0, W = 0, l0 = 0, nl = 0, hi_last = 0;
+    G1Aff* tab = nullptr;
+    uint32_t* offs = nullptr;
+    uint32_t* ents = nullptr;
+  };
+  std::vector<WdClass> wd;
+  int n_l0 = 0, n_lines = 0;
+  int wide_lines() const {
+    int n = 0;
+    for (const WdClass& k : wd) n += k.nl;
+    return n;
+  }
   // free choices of the kernels (zg_ctx_autotune / zg_ctx_set_tuning); the
   // defaults are the fastest on the B200. tuning_gen counts changes, so the
   // request pipeline re-captures its CUDA graphs.
@@ -334,6 +348,44 @@ struct zg_reply {
 
 namespace {
 
+// Wide-window classes of a context with 1024 columns: quotient line l's nodes
+// hold 2^(lr + 9 - l) points and the high line's 2^(lr + 10), so a line takes
+// units of 2^min(15, log2 node) points when its nodes hold more than 1024. A
+// class per unit size, largest first; each class's tables are allocated only
+// with 8 GiB left over for the blob buffers and the request pipeline's slots,
+// and the first class that does not fit ends the list, so the chunk lines stay
+// one contiguous range n_l0 .. n_l0 + n_lines - 1 (the high line last when it
+// has no class).
+void plan_wide_classes(zg_ctx* c) {
+  const int lr = c->lr;
+  int next = 0;  // first quotient line without a class
+  bool high = false;
+  for (int u = WD_MAX_LOG; u >= WD_MIN_LOG; --u) {
+    zg_ctx::WdClass k;
+    k.ulog = u;
+    k.W = wd_windows(u);
+    k.l0 = next;
+    int nq = 0;
+    while (next + nq < lr && std::min(WD_MAX_LOG, lr + 9 - (next + nq)) == u) ++nq;
+    const bool hi = std::min(WD_MAX_LOG, lr + 10) == u;
+    if (!nq && !hi) continue;
+    k.nl = nq + (hi ? 1 : 0);
+    k.hi_last = hi ? 1 : 0;
+    const size_t bytes = (size_t)3 * k.nl * k.W * c->N * sizeof(G1Aff);
+    size_t free_b = 0, total_b = 0;
+    if (cudaMemGetInfo(&free_b, &total_b) != cudaSuccess || free_b < bytes + (8ull << 30) ||
+        cudaMalloc(&k.tab, bytes) != cudaSuccess) {
+      cudaGetLastError();
+      break;
+    }
+    next += nq;
+    high = high || hi;
+    c->wd.push_back(k);
+  }
+  c->n_l0 = next;
+  c->n_lines = lr + 1 - next + (high ? 0 : 1);
+}
+
 int alloc_blob_buffers(zg_ctx* c) {
   const size_t N = c->N, R = c->R;
   if (c->fb) {
@@ -351,19 +403,13 @@ int alloc_blob_buffers(zg_ctx* c) {
       c->fb_ctas[k] = (unsigned)std::max(1, sms * std::max(1, per_sm[k]));
       most = std::max(most, c->fb_ctas[k]);
     }
-    if (c->nwl) {
-      const size_t units = c->N >> WD_UNIT_LOG;
-      ZG_CK(cudaMalloc(&c->wd_offs, 3 * units * (WD_BUCKETS + 1) * sizeof(uint32_t)));
-      ZG_CK(cudaMalloc(&c->wd_ents, 3 * units * WD_UNIT_ENTS * sizeof(uint32_t)));
-      ZG_CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm[0], k_fb_accum<MulImad, true>, FB_ACC_THREADS, 0));
-      ZG_CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm[1], k_fb_accum<MulHybrid, true>, FB_ACC_THREADS, 0));
-      ZG_CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm[2], k_fb_accum<MulF64, true>, FB_ACC_THREADS, 0));
-      for (int k = 0; k < 3; ++k) {
-        c->wd_ctas[k] = (unsigned)std::max(1, sms * std::max(1, per_sm[k]));
-        most = std::max(most, c->wd_ctas[k]);
-      }
+    for (zg_ctx::WdClass& k : c->wd) {
+      const size_t units = c->N >> k.ulog;
+      ZG_CK(cudaMalloc(&k.offs, 3 * units * (((size_t)1 << k.ulog) + 1) * sizeof(uint32_t)));
+      ZG_CK(cudaMalloc(&k.ents, 3 * units * wd_unit_ents(k.ulog) * sizeof(uint32_t)));
     }
     ZG_CK(cudaMalloc(&c->fb_gbuf, (size_t)most * FB_MAX_TASKS * sizeof(XYZZ)));
+    ZG_CK(cudaMalloc(&c->fb_next, sizeof(uint32_t)));
   }
   ZG_CK(cudaMalloc(&c->raw, c->max_blob + 16));
   ZG_CK(cudaMalloc(&c->enc, 3 * N * 32));
@@ -582,53 +628,81 @@ BlobBufs ctx_bufs(zg_ctx* c) {
 // levels, file root, MSM (sort, accumulate, combine or chunks, combine),
 // trees, serialisation, slices.
 uint64_t launches_per_encode(const zg_ctx* c) {
-  return 3 + (uint64_t)c->tree_depth + 1 + 1 + (c->fb ? 3 : 2) + (c->nwl ? 3 : 0) + 1 + 1 + 1;
+  return 3 + (uint64_t)c->tree_depth + 1 + 1 + (c->fb ? 3 : 2) + 2 * c->wd.size() + 1 + 1 + 1;
 }
 
 // the blob MSM's chunk work items: (coset, chunk, line) over the 11-bit
-// tables, for the lines that have no wide windows (nwq .. L - 2, and the high
-// line L - 1 when the context has no wide lines)
+// tables, for the lines without wide windows (n_l0 .. n_l0 + n_lines - 1)
 FbAccArgs blob_fb_args(const zg_ctx* c) {
   FbAccArgs fa;
   fa.tab = c->tab;
   fa.offs = c->fb_offs;
   fa.ents = c->fb_ents;
-  fa.ents32 = nullptr;
   fa.outT = c->fb_T;
   fa.outS = c->fb_S;
   fa.lr = c->lr;
   fa.lc = c->lc;
-  fa.lines = c->L - c->nwl;
-  fa.l0 = c->nwq;
+  fa.lines = c->n_lines;
+  fa.l0 = c->n_l0;
   fa.Ltot = c->L;
+  fa.W = FB_WINDOWS;
   fa.tabN = c->N;
   return fa;
 }
-FbCombineMap blob_fb_map(const zg_ctx* c) { return FbCombineMap{c->lr, c->L - c->nwl, c->nwq, c->L, 0, 0}; }
 
-// the blob MSM's wide work items: (coset, unit block, wide line); their
-// (T, S) partials follow the chunk items' in fb_T / fb_S
-size_t blob_wd_first(const zg_ctx* c) { return (size_t)3 * c->R * (c->L - c->nwl) * FB_ACC_THREADS; }
-FbAccArgs blob_wd_args(const zg_ctx* c) {
+// first item of wide class k in the blob's item order (chunk items, then the
+// classes); the (T, S) partials of item u sit at fb_T / fb_S + 128 u
+uint32_t blob_wd_first_item(const zg_ctx* c, size_t k) {
+  uint32_t u = (uint32_t)(3 * c->R * c->n_lines);
+  for (size_t j = 0; j < k; ++j) u += (uint32_t)(3 * c->R * c->wd[j].nl);
+  return u;
+}
+
+// the blob MSM's work items of wide class k: (coset, unit block, line)
+FbAccArgs blob_wd_args(const zg_ctx* c, size_t k) {
+  const zg_ctx::WdClass& w = c->wd[k];
+  const size_t first = (size_t)blob_wd_first_item(c, k) * FB_ACC_THREADS;
   FbAccArgs fa;
-  fa.tab = c->wtab;
-  fa.offs = c->wd_offs;
-  fa.ents = nullptr;
-  fa.ents32 = c->wd_ents;
-  fa.outT = c->fb_T + blob_wd_first(c);
-  fa.outS = c->fb_S + blob_wd_first(c);
+  fa.tab = w.tab;
+  fa.offs = w.offs;
+  fa.ents32 = w.ents;
+  fa.outT = c->fb_T + first;
+  fa.outS = c->fb_S + first;
   fa.lr = c->lr;
   fa.lc = c->lc;
-  fa.lines = c->nwl;
+  fa.lines = w.nl;
   fa.l0 = 0;
-  fa.Ltot = c->nwl;
+  fa.Ltot = w.nl;
+  fa.ulog = w.ulog;
+  fa.W = w.W;
   fa.tabN = c->N;
   return fa;
 }
-FbCombineMap blob_wd_map(const zg_ctx* c) { return FbCombineMap{c->lr, c->nwl, 0, c->L, 1, 1}; }
 
-// one item set of a single MSM over table line `line` of `tab` (lines = 1)
-FbCombineMap single_fb_map(int lr) { return FbCombineMap{lr, 1, 0, 1, 0, 0}; }
+// the combine plan of a blob: the chunk items, then every wide class
+FbCombinePlan blob_fb_plan(const zg_ctx* c) {
+  FbCombinePlan p;
+  p.n = 1 + (int)c->wd.size();
+  p.start[0] = 0;
+  p.m[0] = FbCombineMap{c->lr, c->n_lines, c->n_l0, c->L, 0, 0};
+  for (size_t k = 0; k < c->wd.size(); ++k) {
+    const zg_ctx::WdClass& w = c->wd[k];
+    p.start[k + 1] = blob_wd_first_item(c, k);
+    p.m[k + 1] = FbCombineMap{c->lr, w.nl, w.l0, c->L, w.hi_last, w.ulog - 10};
+  }
+  p.start[p.n] = blob_wd_first_item(c, c->wd.size());
+  return p;
+}
+
+// the items of a single MSM over one table line (lines = 1)
+FbCombinePlan single_fb_plan(int lr) {
+  FbCombinePlan p;
+  p.n = 1;
+  p.start[0] = 0;
+  p.start[1] = 1u << lr;
+  p.m[0] = FbCombineMap{lr, 1, 0, 1, 0, 0};
+  return p;
+}
 
 // seeded pseudo-random payload bytes (the autotuner's synthetic blob)
 __global__ void k_fill_payload(uint8_t* p, uint64_t n, uint64_t seed) {
@@ -641,30 +715,71 @@ __global__ void k_fill_payload(uint8_t* p, uint64_t n, uint64_t seed) {
   }
 }
 
-// k_fb_accum over `units` work items with product kind `kind` (chunk items,
-// or wide items when `wide`)
-void launch_fb_accum(const zg_ctx* c, uint32_t kind, const FbAccArgs& fa, uint32_t units, cudaStream_t s,
-                     bool wide = false) {
-  const unsigned grid = std::min<unsigned>(wide ? c->wd_ctas[kind] : c->fb_ctas[kind], units);
-  if (wide) {
-    if (kind == ZG_MSM_PRODUCT_IMAD) k_fb_accum<MulImad, true><<<grid, FB_ACC_THREADS, 0, s>>>(fa, c->fb_gbuf, units);
-    else if (kind == ZG_MSM_PRODUCT_FP64) k_fb_accum<MulF64, true><<<grid, FB_ACC_THREADS, 0, s>>>(fa, c->fb_gbuf, units);
-    else k_fb_accum<MulHybrid, true><<<grid, FB_ACC_THREADS, 0, s>>>(fa, c->fb_gbuf, units);
-    return;
+// k_fb_accum over the item sets of `p` with product kind `kind`
+void launch_fb_accum(const zg_ctx* c, uint32_t kind, const FbAccPlan& p, cudaStream_t s) {
+  const uint32_t units = p.start[p.n];
+  const unsigned grid = std::min<unsigned>(c->fb_ctas[kind], units);
+  cudaMemsetAsync(c->fb_next, 0, sizeof(uint32_t), s);
+  if (kind == ZG_MSM_PRODUCT_IMAD) k_fb_accum<MulImad><<<grid, FB_ACC_THREADS, 0, s>>>(p, c->fb_gbuf, c->fb_next);
+  else if (kind == ZG_MSM_PRODUCT_FP64) k_fb_accum<MulF64><<<grid, FB_ACC_THREADS, 0, s>>>(p, c->fb_gbuf, c->fb_next);
+  else k_fb_accum<MulHybrid><<<grid, FB_ACC_THREADS, 0, s>>>(p, c->fb_gbuf, c->fb_next);
+}
+
+// a plan of one item set: the first `units` items of `fa`
+FbAccPlan single_acc_plan(const FbAccArgs& fa, uint32_t units) {
+  FbAccPlan p;
+  p.n = 1;
+  p.start[0] = 0;
+  p.start[1] = units;
+  p.a[0] = fa;
+  return p;
+}
+
+// the blob MSM's items in one plan: the chunk items, then every wide class
+// (the order of blob_fb_plan)
+FbAccPlan blob_acc_plan(const zg_ctx* c) {
+  FbAccPlan p;
+  p.n = 1 + (int)c->wd.size();
+  p.start[0] = 0;
+  p.a[0] = blob_fb_args(c);
+  for (size_t k = 0; k < c->wd.size(); ++k) {
+    p.start[k + 1] = blob_wd_first_item(c, k);
+    p.a[k + 1] = blob_wd_args(c, k);
   }
-  if (kind == ZG_MSM_PRODUCT_IMAD) k_fb_accum<MulImad><<<grid, FB_ACC_THREADS, 0, s>>>(fa, c->fb_gbuf, units);
-  else if (kind == ZG_MSM_PRODUCT_FP64) k_fb_accum<MulF64><<<grid, FB_ACC_THREADS, 0, s>>>(fa, c->fb_gbuf, units);
-  else k_fb_accum<MulHybrid><<<grid, FB_ACC_THREADS, 0, s>>>(fa, c->fb_gbuf, units);
+  p.start[p.n] = blob_wd_first_item(c, c->wd.size());
+  return p;
 }
 
 // P = sum_i T_i + 8 sum_i i S_i per item: one thread per item for a blob's
 // items (fewest additions), one warp per item below 16 384 items
-// (the items' partials start at fb_T / fb_S + first)
-void launch_fb_combine(const zg_ctx* c, uint32_t units, const FbCombineMap& m, cudaStream_t s, size_t first = 0) {
-  const XYZZ* T = c->fb_T + first;
-  const XYZZ* S = c->fb_S + first;
-  if (units >= 16384) k_fb_combine<<<nblk(units, 64), 64, 0, s>>>(T, S, c->part, m, units);
-  else k_fb_combine_warp<<<nblk((size_t)units * 32, 128), 128, 0, s>>>(T, S, c->part, m, units);
+void launch_fb_combine(const zg_ctx* c, const FbCombinePlan& p, cudaStream_t s) {
+  const uint32_t units = p.start[p.n];
+  if (units >= 16384) k_fb_combine<<<nblk(units, 64), 64, 0, s>>>(c->fb_T, c->fb_S, c->part, p);
+  else k_fb_combine_warp<<<nblk((size_t)units * 32, 128), 128, 0, s>>>(c->fb_T, c->fb_S, c->part, p);
+}
+
+// k_wd_sort / k_wd_tables for a class's unit size
+void launch_wd_sort(int ulog, const uint8_t* enc, uint32_t* offs, uint32_t* ents, int lr, int lc, size_t N,
+                    cudaStream_t s) {
+  const dim3 grid((unsigned)(N >> ulog), 3);
+  const size_t sm = wd_sort_smem_bytes(ulog);
+  switch (ulog) {
+    case 15: k_wd_sort<15><<<grid, WD_SORT_THREADS, sm, s>>>(enc, offs, ents, lr, lc, 1, N); break;
+    case 14: k_wd_sort<14><<<grid, WD_SORT_THREADS, sm, s>>>(enc, offs, ents, lr, lc, 1, N); break;
+    case 13: k_wd_sort<13><<<grid, WD_SORT_THREADS, sm, s>>>(enc, offs, ents, lr, lc, 1, N); break;
+    case 12: k_wd_sort<12><<<grid, WD_SORT_THREADS, sm, s>>>(enc, offs, ents, lr, lc, 1, N); break;
+    default: k_wd_sort<11><<<grid, WD_SORT_THREADS, sm, s>>>(enc, offs, ents, lr, lc, 1, N); break;
+  }
+}
+void launch_wd_tables(const zg_ctx* c, const zg_ctx::WdClass& k, cudaStream_t s) {
+  const unsigned g = nblk((uint64_t)3 * k.nl * c->N, 128);
+  switch (k.ulog) {
+    case 15: k_wd_tables<15><<<g, 128, 0, s>>>(k.tab, c->tab, c->N, c->L, k.l0, k.nl, k.hi_last); break;
+    case 14: k_wd_tables<14><<<g, 128, 0, s>>>(k.tab, c->tab, c->N, c->L, k.l0, k.nl, k.hi_last); break;
+    case 13: k_wd_tables<13><<<g, 128, 0, s>>>(k.tab, c->tab, c->N, c->L, k.l0, k.nl, k.hi_last); break;
+    case 12: k_wd_tables<12><<<g, 128, 0, s>>>(k.tab, c->tab, c->N, c->L, k.l0, k.nl, k.hi_last); break;
+    default: k_wd_tables<11><<<g, 128, 0, s>>>(k.tab, c->tab, c->N, c->L, k.l0, k.nl, k.hi_last); break;
+  }
 }
 
 // the three RS-extension passes with a given column tile and block size
@@ -703,15 +818,10 @@ int encode_launches(zg_ctx* c, const BlobBufs& b, size_t len, bool by_device_len
   if (c->fb) {
     k_fb_sort<<<dim3((unsigned)R, 3), 256, fb_sort_smem_bytes(lc), s>>>(b.enc, c->fb_offs, c->fb_ents, lr, lc, 1,
                                                                          N);
-    if (c->nwl)
-      k_wd_sort<<<dim3((unsigned)(N >> WD_UNIT_LOG), 3), WD_SORT_THREADS, wd_sort_smem_bytes(), s>>>(
-          b.enc, c->wd_offs, c->wd_ents, lr, lc, 1, N);
-    const uint32_t units = (uint32_t)(3 * R * (c->L - c->nwl)), wunits = (uint32_t)(3 * R * c->nwl);
-    launch_fb_accum(c, c->msm_product, blob_fb_args(c), units, s);
-    if (c->nwl) launch_fb_accum(c, c->msm_product, blob_wd_args(c), wunits, s, true);
+    for (const zg_ctx::WdClass& k : c->wd) launch_wd_sort(k.ulog, b.enc, k.offs, k.ents, lr, lc, N, s);
+    launch_fb_accum(c, c->msm_product, blob_acc_plan(c), s);
     mark(3);
-    launch_fb_combine(c, units, blob_fb_map(c), s);
-    if (c->nwl) launch_fb_combine(c, wunits, blob_wd_map(c), s, blob_wd_first(c));
+    launch_fb_combine(c, blob_fb_plan(c), s);
   } else {
     MsmChunkArgs a;
     a.scalars = b.enc;
@@ -1437,8 +1547,8 @@ int verify_msms(VerifyRun& v, const bool present[3], XYZZ* out) {
     fa.l0 = 0;
     fa.Ltot = 1;
     fa.tabN = c->N;
-    launch_fb_accum(c, c->msm_product, fa, R, v.s);
-    launch_fb_combine(c, R, single_fb_map(c->lr), v.s);
+    launch_fb_accum(c, c->msm_product, single_acc_plan(fa, R), v.s);
+    launch_fb_combine(c, single_fb_plan(c->lr), v.s);
     k_sum_points<<<1, 256, 0, v.s>>>(c->part, R, out + cs);
   }
   return check_launch();
@@ -1746,22 +1856,9 @@ int zg_ctx_create(const zg_config* cfg, zg_ctx** out) {
   }
   if (!c->tab && cudaMalloc(&c->tab, (size_t)3 * c->L * c->N * sizeof(G1Aff)) != cudaSuccess)
     return bail(fail(ZG_ERR_CUDA, "cannot allocate params"));
-  // wide windows for the lines whose AMT nodes hold >= 2^15 points (auto only;
-  // 1024 columns, so that a unit's 32 blocks are 32 chunks' item slots)
-  // and 8 GiB left over for the blob buffers and the request pipeline's slots
-  size_t free_b = 0, total_b = 0;
-  if (c->fb && wb == 0 && c->lc == 10 && c->lr >= WD_UNIT_LOG - c->lc &&
-      cudaMemGetInfo(&free_b, &total_b) == cudaSuccess) {
-    const int nwq = c->lr + c->lc - WD_UNIT_LOG;
-    const size_t bytes = (size_t)3 * (nwq + 1) * WD_WINDOWS * c->N * sizeof(G1Aff);
-    if (free_b >= bytes + (8ull << 30) && cudaMalloc(&c->wtab, bytes) == cudaSuccess) {
-      c->nwq = nwq;
-      c->nwl = nwq + 1;
-    } else {
-      cudaGetLastError();
-      c->wtab = nullptr;
-    }
-  }
+  c->n_l0 = 0;
+  c->n_lines = c->L;
+  if (c->fb && wb == 0 && c->lc == 10) plan_wide_classes(c);
   if ((rc = alloc_blob_buffers(c))) return bail(rc);
   if (cfg->params_dir && cfg->params_dir[0]) rc = load_mont_params(c, cfg->params_dir);
   else {
@@ -1773,9 +1870,7 @@ int zg_ctx_create(const zg_config* cfg, zg_ctx** out) {
   if (c->fb) {
     const uint64_t nl = (uint64_t)3 * c->L;
     k_fb_tables<<<nblk(nl * c->N, 128), 128, 0, c->stream>>>(c->tab, c->N, nl);
-    if (c->nwl)
-      k_wd_tables<<<nblk((uint64_t)3 * c->nwl * c->N, 128), 128, 0, c->stream>>>(c->wtab, c->tab, c->N, c->L, c->nwq,
-                                                                                  c->nwl);
+    for (const zg_ctx::WdClass& k : c->wd) launch_wd_tables(c, k, c->stream);
     if (cudaStreamSynchronize(c->stream) != cudaSuccess || cudaGetLastError() != cudaSuccess)
       return bail(fail(ZG_ERR_CUDA, "fixed-base table build failed"));
   }
@@ -1796,8 +1891,12 @@ void zg_ctx_destroy(zg_ctx* c) {
   if (c->h_rec) cudaFreeHost(c->h_rec);
   void* ps[] = {c->tab, c->raw, c->enc, c->T1, c->Bc, c->win, c->part, c->nodes, c->amt,
                 c->tree, c->tree_off_d, c->slices, c->file_root, c->fb_offs, c->fb_ents, c->fb_T, c->fb_S, c->fb_gbuf,
-                c->wtab, c->wd_offs, c->wd_ents};
+                c->fb_next};
   for (void* p : ps) if (p) cudaFree(p);
+  for (zg_ctx::WdClass& k : c->wd) {
+    void* w[] = {k.tab, k.offs, k.ents};
+    for (void* p : w) if (p) cudaFree(p);
+  }
   if (c->h_in) cudaFreeHost(c->h_in);
   for (cudaEvent_t e : c->ev) if (e) cudaEventDestroy(e);
   if (c->done) cudaEventDestroy(c->done);
@@ -2189,7 +2288,7 @@ int zg_ctx_get_tuning(zg_ctx* c, zg_tuning* out) {
   out->msm_product = c->msm_product;
   out->ntt_cols_per_cta = c->ntt_cpb;
   out->ntt_threads = c->ntt_threads;
-  out->msm_wide_lines = (uint32_t)c->nwl;
+  out->msm_wide_lines = (uint32_t)c->wide_lines();
   return ZG_OK;
 }
 
@@ -2245,15 +2344,16 @@ int zg_ctx_autotune(zg_ctx* c, zg_tuning* out) {
   if (c->fb) {
     // a sample of the chunk items and of the wide items: the first 4 per
     // resident CTA of each
-    const uint32_t all = (uint32_t)(3 * c->R * (c->L - c->nwl)), wall = (uint32_t)(3 * c->R * c->nwl);
+    const uint32_t all = (uint32_t)(3 * c->R * c->n_lines);
+    const uint32_t wall = c->wd.empty() ? 0u : (uint32_t)(3 * c->R * c->wd[0].nl);
     const uint32_t sample = std::min<uint32_t>(all, 4 * std::max(c->fb_ctas[0], std::max(c->fb_ctas[1], c->fb_ctas[2])));
-    const uint32_t wsample = std::min<uint32_t>(wall, 4 * std::max(c->wd_ctas[0], std::max(c->wd_ctas[1], c->wd_ctas[2])));
-    const FbAccArgs fa = blob_fb_args(c), fw = blob_wd_args(c);
+    const uint32_t wsample = std::min<uint32_t>(wall, 4 * std::max(c->fb_ctas[0], std::max(c->fb_ctas[1], c->fb_ctas[2])));
+    const FbAccArgs fa = blob_fb_args(c), fw = c->wd.empty() ? FbAccArgs() : blob_wd_args(c, 0);
     float best = 0;
     for (uint32_t k = 0; k < 3; ++k) {
       t.msm_ms[k] = timed([&] {
-        launch_fb_accum(c, k, fa, sample, s);
-        if (wsample) launch_fb_accum(c, k, fw, wsample, s, true);
+        launch_fb_accum(c, k, single_acc_plan(fa, sample), s);
+        if (wsample) launch_fb_accum(c, k, single_acc_plan(fw, wsample), s);
       });
       if (t.msm_ms[k] > 0 && (best == 0 || t.msm_ms[k] < best)) { best = t.msm_ms[k]; best_msm = k; }
     }
@@ -2280,7 +2380,7 @@ int zg_ctx_autotune(zg_ctx* c, zg_tuning* out) {
   t.msm_product = best_msm;
   t.ntt_cols_per_cta = best_cpb;
   t.ntt_threads = best_th;
-  t.msm_wide_lines = (uint32_t)c->nwl;
+  t.msm_wide_lines = (uint32_t)c->wide_lines();
   if (out) *out = t;
   return ZG_OK;
 }
@@ -2507,8 +2607,8 @@ int zg_ctx_msm(zg_ctx* c, uint32_t coset, uint32_t line, const void* d_scalars, 
   fa.l0 = 0;
   fa.Ltot = 1;
   fa.tabN = c->N;
-  launch_fb_accum(c, c->msm_product, fa, nch, s);
-  launch_fb_combine(c, nch, single_fb_map(lrn), s);
+  launch_fb_accum(c, c->msm_product, single_acc_plan(fa, nch), s);
+  launch_fb_combine(c, single_fb_plan(lrn), s);
   k_sum_points<<<1, 256, 0, s>>>(c->part, nch, c->nodes);
   k_serialize_nodes<<<1, 128, 0, s>>>(c->nodes, (uint8_t*)d_out, 1);
   c->launches += 5;

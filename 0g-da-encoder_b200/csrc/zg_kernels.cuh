@@ -363,22 +363,25 @@ constexpr int FB_BUCKETS = 1 << (FB_BITS - 1);    // 1024
 constexpr int FB_ACC_THREADS = 128;
 constexpr int FB_PER_THREAD = FB_BUCKETS / FB_ACC_THREADS;  // 8 buckets per thread
 
-// Wide windows for the AMT lines whose nodes are MSMs over >= 2^15 points: a
-// node's 2^15-point sort units share 2^15 buckets of 16-bit signed digits, so
-// a point costs 16 bucket additions instead of 24 and the bucket reduction is
-// paid per unit instead of per 1024-point chunk. A unit's buckets are cut into
-// 32 blocks of FB_BUCKETS, each block one work item of k_fb_accum: with 1024
-// columns a (coset, line) still has exactly R items, item u * 32 + blk = block
-// blk of unit u, and a node's items are contiguous, so the AMT tree kernel
-// sums them like chunk results.
-constexpr int WD_BITS = 16;
-constexpr int WD_WINDOWS = 16;                         // 256 bits; the top digit of a scalar < r is < 2^14
-constexpr int WD_BUCKETS = 1 << (WD_BITS - 1);         // |digit| in 1 .. 2^15
-constexpr int WD_UNIT_LOG = 15;                        // points per sort unit
-constexpr int WD_UNIT = 1 << WD_UNIT_LOG;
-constexpr int WD_BLOCKS = WD_BUCKETS / FB_BUCKETS;     // 32 work items per unit
-constexpr uint64_t WD_UNIT_ENTS = (uint64_t)WD_UNIT * WD_WINDOWS;  // entry capacity of a unit
-static_assert(WD_BLOCKS * 1024 == WD_UNIT, "a unit's items are 32 chunks' worth (1024 columns)");
+// Wide windows for the AMT lines whose nodes are MSMs over more than 1024
+// points. Such a line's nodes are cut into sort units of U = 2^ulog points
+// (11 <= ulog <= 15, U <= the node size) that share U buckets of signed
+// (ulog + 1)-bit digits: W = floor(254 / c) + 1 windows of c = ulog + 1 bits,
+// i.e. 16 bucket additions per point at U = 2^15 instead of 24, and the bucket
+// reduction paid per unit instead of per 1024-point chunk. A unit's buckets
+// are cut into U / 1024 blocks of FB_BUCKETS, each block one work item of
+// k_fb_accum: with 1024 columns a (coset, line) still has exactly R items,
+// item u * (U / 1024) + blk = block blk of unit u, and a node's items are
+// contiguous, so the AMT tree kernel sums them like chunk results.
+constexpr int WD_MIN_LOG = 11;
+constexpr int WD_MAX_LOG = 15;
+__host__ __device__ constexpr int wd_windows(int ulog) { return 254 / (ulog + 1) + 1; }
+// The top digit of a scalar < r never carries out: (r - 1) >> ((W - 1) c) + 1
+// < 2^(c - 1) for every c = 12 .. 16 (top values 3, 96, 3, 12388, 12388).
+static_assert(wd_windows(15) == 16 && wd_windows(14) == 17 && wd_windows(13) == 19 && wd_windows(12) == 20 &&
+                  wd_windows(11) == 22,
+              "window counts");
+__host__ __device__ constexpr uint64_t wd_unit_ents(int ulog) { return (uint64_t)wd_windows(ulog) << ulog; }
 
 // col[(w + 1) * N] = 2^(BITS (w + 1)) * col[0] for w < WIN - 1: BITS
 // doublings per window, then one batch inversion for the affine conversions.
@@ -419,19 +422,22 @@ __global__ void __launch_bounds__(128) k_fb_tables(G1Aff* tab, uint64_t N, uint6
   fb_fill_windows<FB_BITS, FB_WINDOWS>(tab + line * FB_WINDOWS * N + p, N);
 }
 
-// Wide-window tables of the wide lines: wtab[((cs * nwl + wl) * WD_WINDOWS + w) * N + p]
-// = 2^(16 w) P with P = point p of AMT line (wl < nwq ? wl : L - 1) of coset
-// cs, read from window 0 of the 11-bit table tab[cs][line][FB_WINDOWS][N].
+// Wide-window tables of a class of nl lines of unit 2^ULOG:
+// wtab[((cs * nl + wl) * W + w) * N + p] = 2^(c w) P, P = point p of AMT line
+// (hi_last && wl == nl - 1 ? L - 1 : l0 + wl) of coset cs, read from window 0
+// of the 11-bit table tab[cs][line][FB_WINDOWS][N].
+template <int ULOG>
 __global__ void __launch_bounds__(128) k_wd_tables(G1Aff* wtab, const G1Aff* __restrict__ tab, uint64_t N, int L,
-                                                   int nwq, int nwl) {
+                                                   int l0, int nl, int hi_last) {
+  constexpr int W = wd_windows(ULOG);
   uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= 3ull * nwl * N) return;
-  const uint64_t p = i % N, cl = i / N;  // cl = cs * nwl + wl
-  const int wl = (int)(cl % nwl), cs = (int)(cl / nwl);
-  const int line = wl < nwq ? wl : L - 1;
-  G1Aff* col = wtab + cl * WD_WINDOWS * N + p;
+  if (i >= 3ull * nl * N) return;
+  const uint64_t p = i % N, cl = i / N;  // cl = cs * nl + wl
+  const int wl = (int)(cl % nl), cs = (int)(cl / nl);
+  const int line = (hi_last && wl == nl - 1) ? L - 1 : l0 + wl;
+  G1Aff* col = wtab + cl * W * N + p;
   col[0] = tab[((uint64_t)cs * L + line) * FB_WINDOWS * N + p];
-  fb_fill_windows<WD_BITS, WD_WINDOWS>(col, N);
+  fb_fill_windows<ULOG + 1, W>(col, N);
 }
 
 // signed 11-bit digit w of a scalar given as 8 little-endian u32 limbs
@@ -527,62 +533,72 @@ __global__ void __launch_bounds__(256) k_fb_sort(const uint8_t* __restrict__ sca
 }
 
 constexpr int WD_SORT_THREADS = 1024;
-inline size_t wd_sort_smem_bytes() { return (size_t)(WD_BUCKETS + 1 + 32) * sizeof(uint32_t); }
+inline size_t wd_sort_smem_bytes(int ulog) { return (size_t)((1u << ulog) + 1 + 32) * sizeof(uint32_t); }
 
-// Per wide sort unit (2^15 consecutive points of a coset, i.e. chunks
-// 32 u .. 32 u + 31 of 1024 columns): counting sort of the (point, window)
-// pairs by |digit| of the signed 16-bit digits.
+// Per sort unit of U = 2^ULOG consecutive points of a coset (chunks
+// u U / 1024 .. (u + 1) U / 1024 - 1 of 1024 columns): counting sort of the
+// (point, window) pairs by |digit| of the signed c = ULOG + 1 bit digits.
 //   offs[cs][u][k] .. offs[cs][u][k + 1] = entries of bucket k (|digit| = k + 1)
-//   ents[cs][u][e] = p | w << 15 | sign << 31, p the point within the unit
-// Point p of unit u is chunk b = (u << 5) + (p >> 10), element t = p & 1023,
-// read like k_fb_sort reads it. Pass 1 counts, a block scan turns the counts
-// into fill pointers, pass 2 scatters (the scalars are read twice).
+//   ents[cs][u][e] = p | w << ULOG | sign << 31, p the point within the unit
+// Point p of unit u is chunk b = (u U + p) >> lc, element t = (u U + p) &
+// (2^lc - 1), read like k_fb_sort reads it. Pass 1 counts, a block scan turns
+// the counts into fill pointers, pass 2 scatters (the scalars are read twice).
+template <int C>
 __device__ __forceinline__ uint32_t wd_window_bits(const uint32_t* s, int w) {
-  return (s[w >> 1] >> ((w & 1) << 4)) & 0xffffu;
+  const int o = C * w;
+  const int li = o >> 5, sh = o & 31;
+  uint32_t v = s[li] >> sh;
+  if (sh > 32 - C && li + 1 < 8) v |= s[li + 1] << (32 - sh);
+  return v & ((1u << C) - 1);
 }
 
+template <int ULOG>
 __global__ void __launch_bounds__(WD_SORT_THREADS) k_wd_sort(const uint8_t* __restrict__ scalars,
                                                              uint32_t* __restrict__ offs, uint32_t* __restrict__ ents,
                                                              int lr, int lc, int bitrev_rows,
                                                              uint64_t scalar_coset_stride) {
-  extern __shared__ __align__(16) uint32_t wcnt[];  // [WD_BUCKETS + 1], then [32] warp sums
-  uint32_t* wsum = wcnt + WD_BUCKETS + 1;
+  constexpr int C = ULOG + 1, W = wd_windows(ULOG);
+  constexpr uint32_t U = 1u << ULOG, NB = U;           // buckets = 2^(c - 1) = U
+  constexpr int PER = (int)NB / WD_SORT_THREADS;       // counters per thread in the scan
+  static_assert(PER >= 1, "at least 1024 buckets");
+  extern __shared__ __align__(16) uint32_t wcnt[];     // [NB + 1], then [32] warp sums
+  uint32_t* wsum = wcnt + NB + 1;
   const uint32_t unit = blockIdx.x, coset = blockIdx.y, nunits = gridDim.x;
-  const uint32_t C = 1u << lc;
+  const uint32_t Cn = 1u << lc;
   const uint8_t* src = scalars + scalar_coset_stride * coset * 32;
-  uint32_t* o = offs + ((size_t)coset * nunits + unit) * (WD_BUCKETS + 1);
-  uint32_t* e = ents + ((size_t)coset * nunits + unit) * WD_UNIT_ENTS;
-  for (int k = threadIdx.x; k <= WD_BUCKETS; k += blockDim.x) wcnt[k] = 0;
+  uint32_t* o = offs + ((size_t)coset * nunits + unit) * (NB + 1);
+  uint32_t* e = ents + ((size_t)coset * nunits + unit) * wd_unit_ents(ULOG);
+  for (uint32_t k = threadIdx.x; k <= NB; k += blockDim.x) wcnt[k] = 0;
   __syncthreads();
   for (int pass = 0; pass < 2; ++pass) {
-    for (uint32_t p = threadIdx.x; p < (uint32_t)WD_UNIT; p += blockDim.x) {
-      const uint32_t gp = (unit << WD_UNIT_LOG) + p;
-      const uint32_t b = gp >> lc, t = gp & (C - 1);
+    for (uint32_t p = threadIdx.x; p < U; p += blockDim.x) {
+      const uint32_t gp = (unit << ULOG) + p;
+      const uint32_t b = gp >> lc, t = gp & (Cn - 1);
       const uint32_t row = bitrev_rows ? brev_bits(b, lr) : b;
       const uint32_t col = bitrev_rows ? brev_bits(t, lc) : t;
-      const uint4* q = reinterpret_cast<const uint4*>(src + ((uint64_t)row * C + col) * 32);
+      const uint4* q = reinterpret_cast<const uint4*>(src + ((uint64_t)row * Cn + col) * 32);
       const uint4 x = q[0], y = q[1];
       const uint32_t s[8] = {x.x, x.y, x.z, x.w, y.x, y.y, y.z, y.w};
       uint32_t carry = 0;
 #pragma unroll
-      for (int w = 0; w < WD_WINDOWS; ++w) {
-        const uint32_t v = wd_window_bits(s, w) + carry;
+      for (int w = 0; w < W; ++w) {
+        const uint32_t v = wd_window_bits<C>(s, w) + carry;
         uint32_t mag, neg;
-        if (v >= (uint32_t)WD_BUCKETS) { mag = (1u << WD_BITS) - v; neg = 1; carry = 1; }
+        if (v >= NB) { mag = (1u << C) - v; neg = 1; carry = 1; }
         else { mag = v; neg = 0; carry = 0; }
         if (mag) {
           const uint32_t pos = atomicAdd(&wcnt[mag - 1], 1u);
-          if (pass) e[pos] = p | (uint32_t)w << WD_UNIT_LOG | neg << 31;
+          if (pass) e[pos] = p | (uint32_t)w << ULOG | neg << 31;
         }
       }
     }
     __syncthreads();
     if (pass == 0) {
-      // exclusive scan of the 2^15 counts: 32 per thread, warp scans, warp sums
+      // exclusive scan of the NB counts: PER per thread, warp scans, warp sums
       const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-      const int k0 = threadIdx.x * (WD_BUCKETS / WD_SORT_THREADS);
+      const int k0 = threadIdx.x * PER;
       uint32_t sum = 0;
-      for (int i = 0; i < WD_BUCKETS / WD_SORT_THREADS; ++i) sum += wcnt[k0 + i];
+      for (int i = 0; i < PER; ++i) sum += wcnt[k0 + i];
       uint32_t incl = sum;
       for (int d = 1; d < 32; d <<= 1) {
         const uint32_t v = __shfl_up_sync(0xffffffffu, incl, d);
@@ -601,20 +617,20 @@ __global__ void __launch_bounds__(WD_SORT_THREADS) k_wd_sort(const uint8_t* __re
       }
       __syncthreads();
       uint32_t acc = wsum[warp] + incl - sum;
-      for (int i = 0; i < WD_BUCKETS / WD_SORT_THREADS; ++i) {
+      for (int i = 0; i < PER; ++i) {
         const uint32_t v = wcnt[k0 + i];
         wcnt[k0 + i] = acc;
         o[k0 + i] = acc;
         acc += v;
       }
-      if (threadIdx.x == blockDim.x - 1) o[WD_BUCKETS] = acc;
+      if (threadIdx.x == blockDim.x - 1) o[NB] = acc;
       __syncthreads();
     }
   }
 }
 
 struct FbAccArgs {
-  const G1Aff* tab = nullptr;      // [cosets][Ltot][W][tabN], W = FB_WINDOWS (WD_WINDOWS for wide items)
+  const G1Aff* tab = nullptr;      // [cosets][Ltot][W][tabN]
   const uint32_t* offs = nullptr;
   const uint16_t* ents = nullptr;    // chunk items
   const uint32_t* ents32 = nullptr;  // wide items (k_wd_sort's lists)
@@ -622,6 +638,8 @@ struct FbAccArgs {
   XYZZ* outS = nullptr;
   int lr = 0, lc = 0, lines = 1;   // 2^lr items of each of `lines` lines per coset
   int l0 = 0, Ltot = 1;            // item line l reads table line l0 + l of Ltot per coset
+  int ulog = 10;                   // wide items: units of 2^ulog points
+  int W = FB_WINDOWS;              // windows per table line (wd_windows(ulog) for wide items)
   uint64_t tabN = 0;               // points per window table (the param line length)
 };
 
@@ -637,37 +655,66 @@ struct FbAccArgs {
 //  3. task partial sums go to this CTA's scratch (gpart, L2-resident);
 //  4. thread i merges the partials of buckets 8i+1 .. 8i+8 and folds them
 //     into running sums S_i = sum B_k, T_i = sum (k - 8i) B_k.
-// WIDE items are 1024-bucket blocks of a wide sort unit (k_wd_sort): item g of
-// a coset is block g & 31 of unit g >> 5, its buckets' entries index the
-// unit's 2^15 points and 16 windows of the wide table.
+// Wide items (ents32 set) are 1024-bucket blocks of a wide sort unit of
+// 2^ulog points (k_wd_sort): item g of a coset is block g & (2^(ulog - 10) -
+// 1) of unit g >> (ulog - 10); its buckets' entries index the unit's points
+// and the W windows of the wide table.
+// One launch covers up to FB_MAX_SETS item sets (a blob's chunk items and its
+// wide classes): set k holds items start[k] .. start[k + 1] - 1, described by
+// a[k] with local item index u - start[k]. One launch keeps the persistent
+// CTAs busy to the end of the whole MSM instead of leaving a partial last
+// round per set. A CTA takes its next item from the counter *next (zero at
+// launch): items differ in size (a wide unit's block 0 holds the top
+// window's digits), and a fixed item-to-CTA map would give some CTAs every
+// heavy item.
+constexpr int FB_MAX_SETS = 8;
+struct FbAccPlan {
+  int n = 0;
+  uint32_t start[FB_MAX_SETS + 1] = {};
+  FbAccArgs a[FB_MAX_SETS];
+};
 constexpr int FB_TASK = 32;
 constexpr int FB_MAX_TASKS = FB_BUCKETS + FB_WINDOWS * 1024 / FB_TASK;  // chunk <= 1024 points
 // M is the product kind of the point additions (MulImad / MulHybrid / MulF64,
 // chosen by the context's tuning; identical results).
-template <class M, bool WIDE = false>
-__global__ void __launch_bounds__(FB_ACC_THREADS, 4) k_fb_accum(FbAccArgs a, XYZZ* __restrict__ gpart_all,
-                                                                uint32_t units) {
+template <class M>
+__global__ void __launch_bounds__(FB_ACC_THREADS, 4) k_fb_accum(const FbAccPlan plan, XYZZ* __restrict__ gpart_all,
+                                                                uint32_t* __restrict__ next) {
   __shared__ uint32_t soffs[FB_BUCKETS + 1];
   __shared__ uint16_t tstart[FB_BUCKETS + 1];
   __shared__ uint16_t order[FB_MAX_TASKS];
   __shared__ uint16_t tbucket[FB_MAX_TASKS];
   __shared__ uint32_t bins[FB_TASK + 1];
+  __shared__ uint32_t item;
   XYZZ* gpart = gpart_all + (size_t)blockIdx.x * FB_MAX_TASKS;
-  const uint32_t nch = 1u << a.lr;
-  const uint64_t N = a.tabN;
-  for (uint32_t u = blockIdx.x; u < units; u += gridDim.x) {
+  const uint32_t units = plan.start[plan.n];
+  for (;;) {
+    __syncthreads();  // every thread has read the previous item number
+    if (threadIdx.x == 0) item = atomicAdd(next, 1u);
+    __syncthreads();
+    const uint32_t gu = item;
+    if (gu >= units) break;
+    int set = 0;
+    while (set + 1 < plan.n && gu >= plan.start[set + 1]) ++set;
+    const FbAccArgs& a = plan.a[set];
+    const uint32_t u = gu - plan.start[set];
+    const uint32_t nch = 1u << a.lr;
+    const uint64_t N = a.tabN;
     const uint32_t l = u % a.lines, g = u / a.lines;
     const uint32_t coset = g / nch, b = g % nch;
     const uint32_t* offs;
     const uint16_t* ents = nullptr;
-    const uint32_t* ents32 = nullptr;
+    const uint32_t* ents32 = a.ents32;
+    const bool wide = ents32 != nullptr;
+    const uint32_t ulog = (uint32_t)a.ulog;
     const G1Aff* tabl;
-    if constexpr (WIDE) {
-      const uint32_t unit = b / WD_BLOCKS, blk = b % WD_BLOCKS;
-      const size_t cu = (size_t)coset * (nch / WD_BLOCKS) + unit;
-      offs = a.offs + cu * (WD_BUCKETS + 1) + (size_t)blk * FB_BUCKETS;
-      ents32 = a.ents32 + cu * WD_UNIT_ENTS;
-      tabl = a.tab + ((uint64_t)coset * a.Ltot + a.l0 + l) * WD_WINDOWS * N + ((uint64_t)unit << WD_UNIT_LOG);
+    if (wide) {
+      const int bl = a.ulog - 10;
+      const uint32_t unit = b >> bl, blk = b & ((1u << bl) - 1);
+      const size_t cu = (size_t)coset * (nch >> bl) + unit;
+      offs = a.offs + cu * ((1u << a.ulog) + 1) + (size_t)blk * FB_BUCKETS;
+      ents32 += cu * wd_unit_ents(a.ulog);
+      tabl = a.tab + ((uint64_t)coset * a.Ltot + a.l0 + l) * a.W * N + ((uint64_t)unit << a.ulog);
     } else {
       offs = a.offs + (size_t)g * (FB_BUCKETS + 1);
       ents = a.ents + (size_t)g * FB_WINDOWS * (1u << a.lc);
@@ -738,17 +785,19 @@ __global__ void __launch_bounds__(FB_ACC_THREADS, 4) k_fb_accum(FbAccArgs a, XYZ
       const uint32_t e1 = min(e0 + tsz, soffs[k + 1]);
       XYZZ B = XYZZ::inf();
       for (uint32_t e = e0; e < e1; ++e) {
-        G1Aff p;
-        bool neg;
-        if constexpr (WIDE) {
+        uint32_t idx, w, neg;
+        if (wide) {
           const uint32_t v = ents32[e];
-          p = load_aff(tabl + (uint64_t)((v >> WD_UNIT_LOG) & (WD_WINDOWS - 1)) * N + (v & (WD_UNIT - 1)));
+          idx = v & ((1u << ulog) - 1);
+          w = (v >> ulog) & 31;
           neg = v >> 31;
         } else {
           const uint32_t v = ents[e];
-          p = load_aff(tabl + (uint64_t)((v >> 10) & 31) * N + (v & 0x3ff));
-          neg = v & 0x8000;
+          idx = v & 0x3ff;
+          w = (v >> 10) & 31;
+          neg = v >> 15;
         }
+        G1Aff p = load_aff(tabl + (uint64_t)w * N + idx);
         if (neg) p.y = -p.y;
         B.template add_affine<M>(p.x, p.y);
       }
@@ -766,20 +815,41 @@ __global__ void __launch_bounds__(FB_ACC_THREADS, 4) k_fb_accum(FbAccArgs a, XYZ
   }
 }
 
-// Where a launch's items go: item u of line l = u % lines (g = u / lines,
+// Where a combine launch's items go. The launch covers up to FB_MAX_SETS item
+// sets (the chunk items, then one set per wide unit size); set k holds items
+// start[k] .. start[k + 1] - 1, whose (T, S) partials sit at the same
+// positions. Local item v = u - start[k] of line l = v % lines (g = v / lines,
 // coset g >> lr, b = g & (2^lr - 1)) is written to part[(coset * L + line) *
-// 2^lr + b], line = L - 1 for the launch's last line when hi_last, else l0 + l.
-// Wide items (block blk = b & 31 of a wide unit) add 1024 blk * sum_k B_k:
-// their buckets hold digits 1024 blk + k + 1.
+// 2^lr + b], line = L - 1 for the set's last line when hi_last, else l0 + l.
+// Wide items (block blk = b & (2^bpu_log - 1) of a unit) add 1024 blk *
+// sum_k B_k: their buckets hold digits 1024 blk + k + 1 (bpu_log = 0 for
+// chunk items).
 struct FbCombineMap {
-  int lr, lines, l0, L, hi_last, wide;
+  int lr, lines, l0, L, hi_last, bpu_log;
+};
+struct FbCombinePlan {
+  int n = 0;
+  uint32_t start[FB_MAX_SETS + 1] = {};
+  FbCombineMap m[FB_MAX_SETS] = {};
 };
 
-__device__ __forceinline__ size_t fb_part_index(const FbCombineMap& m, uint32_t u) {
-  const uint32_t l = u % m.lines, g = u / m.lines;
+// the set of item u, its map and its local index
+__device__ __forceinline__ const FbCombineMap& fb_plan_item(const FbCombinePlan& p, uint32_t u, uint32_t* v) {
+  int k = 0;
+  while (k + 1 < p.n && u >= p.start[k + 1]) ++k;
+  *v = u - p.start[k];
+  return p.m[k];
+}
+
+__device__ __forceinline__ size_t fb_part_index(const FbCombineMap& m, uint32_t v) {
+  const uint32_t l = v % m.lines, g = v / m.lines;
   const uint32_t nch = 1u << m.lr;
   const uint32_t line = (m.hi_last && l == (uint32_t)m.lines - 1) ? (uint32_t)m.L - 1 : (uint32_t)m.l0 + l;
   return ((size_t)(g / nch) * m.L + line) * nch + (g % nch);
+}
+
+__device__ __forceinline__ uint32_t fb_item_block(const FbCombineMap& m, uint32_t v) {
+  return (v / m.lines) & ((1u << m.bpu_log) - 1);
 }
 
 // (1024 blk) * P for blk < 32
@@ -798,9 +868,11 @@ __device__ XYZZ fb_block_term(const XYZZ& P, uint32_t blk) {
 // Per item: P = sum_i T_i + 8 * sum_i i S_i (+ the wide block term); written
 // to part for the AMT trees.
 __global__ void __launch_bounds__(64) k_fb_combine(const XYZZ* __restrict__ T, const XYZZ* __restrict__ S,
-                                                   XYZZ* __restrict__ part, FbCombineMap m, uint32_t count) {
+                                                   XYZZ* __restrict__ part, FbCombinePlan plan) {
   const uint32_t u = blockIdx.x * blockDim.x + threadIdx.x;
-  if (u >= count) return;
+  if (u >= plan.start[plan.n]) return;
+  uint32_t v;
+  const FbCombineMap& m = fb_plan_item(plan, u, &v);
   const XYZZ* t = T + (size_t)u * FB_ACC_THREADS;
   const XYZZ* s = S + (size_t)u * FB_ACC_THREADS;
   XYZZ tot = XYZZ::inf(), run = XYZZ::inf(), wsum = XYZZ::inf();
@@ -812,14 +884,12 @@ __global__ void __launch_bounds__(64) k_fb_combine(const XYZZ* __restrict__ T, c
 #pragma unroll 1
   for (int k = 0; k < 3; ++k) wsum = wsum.dbl();  // x FB_PER_THREAD = 8
   tot.add(wsum);
-  if (m.wide) {
-    const uint32_t blk = (u / m.lines) % WD_BLOCKS;
-    if (blk) {
-      run.add(load_xyzz(s));  // sum of all the item's buckets
-      tot.add(fb_block_term(run, blk));
-    }
+  const uint32_t blk = fb_item_block(m, v);
+  if (blk) {
+    run.add(load_xyzz(s));  // sum of all the item's buckets
+    tot.add(fb_block_term(run, blk));
   }
-  store_xyzz(part + fb_part_index(m, u), tot);
+  store_xyzz(part + fb_part_index(m, v), tot);
 }
 
 __device__ __forceinline__ XYZZ shfl_xor_xyzz(const XYZZ& p, int m) {
@@ -842,11 +912,13 @@ __device__ __forceinline__ XYZZ shfl_xor_xyzz(const XYZZ& p, int m) {
 // lanes l >= 1 of the suffix sums U_l = sum_{m >= l} s_m (a warp scan). About
 // three times the additions of k_fb_combine, so blob encodes keep that one.
 __global__ void __launch_bounds__(128) k_fb_combine_warp(const XYZZ* __restrict__ T, const XYZZ* __restrict__ S,
-                                                         XYZZ* __restrict__ part, FbCombineMap m, uint32_t count) {
+                                                         XYZZ* __restrict__ part, FbCombinePlan plan) {
   static_assert(FB_ACC_THREADS == 128, "four partials per lane");
   const uint32_t u = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   const int lane = threadIdx.x & 31;
-  if (u >= count) return;  // uniform per warp
+  if (u >= plan.start[plan.n]) return;  // uniform per warp
+  uint32_t v;
+  const FbCombineMap& m = fb_plan_item(plan, u, &v);
   const XYZZ* t = T + (size_t)u * FB_ACC_THREADS + 4 * lane;
   const XYZZ* s = S + (size_t)u * FB_ACC_THREADS + 4 * lane;
   XYZZ tl = load_xyzz(t);
@@ -873,11 +945,9 @@ __global__ void __launch_bounds__(128) k_fb_combine_warp(const XYZZ* __restrict_
     a.add(w);                 // sum_i i S_i
     a = a.dbl().dbl().dbl();  // x FB_PER_THREAD = 8
     tl.add(a);
-    if (m.wide) {
-      const uint32_t blk = (u / m.lines) % WD_BLOCKS;
-      if (blk) tl.add(fb_block_term(U, blk));  // U at lane 0 = sum of all the item's buckets
-    }
-    store_xyzz(part + fb_part_index(m, u), tl);
+    const uint32_t blk = fb_item_block(m, v);
+    if (blk) tl.add(fb_block_term(U, blk));  // U at lane 0 = sum of all the item's buckets
+    store_xyzz(part + fb_part_index(m, v), tl);
   }
 }
 

@@ -318,16 +318,18 @@ def test_device_encode_then_host_encode_are_ordered(gpu_pkg, oracle):
 
 @pytest.mark.parametrize("log_row", [5, 6])
 def test_encode_wide_windows_match_oracle(gpu_pkg, oracle, log_row):
-    """With 1024 columns the AMT lines whose nodes hold >= 2^15 points run on
-    16-bit fixed-base windows over 2^15-point units (32 rows: the high line;
-    64 rows: also quotient line 0). Both a random payload and a constant one
-    (every data scalar equal: whole units in one bucket per window, the
-    adaptive task size of the bucket kernel) give the oracle's bytes, and the
-    11-bit-only context gives the same reply."""
+    """With 1024 columns every AMT line whose nodes hold more than 1024 points
+    runs on wide fixed-base windows: units of 2^min(15, log2 node) points and
+    (log2 unit + 1)-bit digits. At 32 and 64 rows all five unit sizes
+    (2^11 .. 2^15) occur; only the last quotient line and the basis line stay
+    on 1024-point chunks. Both a random payload and a constant one (every data
+    scalar equal: whole units in one bucket per window, the adaptive task size
+    of the bucket kernel) give the oracle's bytes, and the 11-bit-only context
+    gives the same reply."""
     seed = 41
     params = gpu_pkg.ZgEncoderParams.from_seed(log_row, 10, seed)
     narrow = gpu_pkg.ZgEncoderParams.from_seed(log_row, 10, seed, msm_window_bits=11)
-    assert params.tuning()["msm_wide_lines"] == log_row - 4
+    assert params.tuning()["msm_wide_lines"] == log_row  # L - 2 of the L = log_row + 2 lines
     assert narrow.tuning()["msm_wide_lines"] == 0
     op = oracle.params(log_row, 10, seed)
     d = params.dims
