@@ -68,6 +68,22 @@ CONFIG = {
 }
 
 
+def executed_mixed_adds(lr, lc):
+    """Bucket additions of table points this build runs per blob (random
+    scalars): the lines whose nodes are single chunks use 24 windows per
+    point; with 1024 columns every other line uses units of 2^min(15, log2
+    node) points and floor(254 / c) + 1 windows of c = log2 unit + 1 bits."""
+    n, total = 1 << (lr + lc), 0
+    for line in range(lr + 2):
+        node = n if line == lr + 1 else (1 << lc if line == lr else n >> (line + 1))
+        if lc == 10 and node > 1024:
+            u = min(15, node.bit_length() - 1)
+            total += 3 * n * (254 // (u + 1) + 1)
+        else:
+            total += 3 * n * 24
+    return total
+
+
 def set_dims(lr, lc):
     """Switch the module constants to another blob shape (profiling runs)."""
     global LOG_ROW, LOG_COL, R, N, PAYLOAD, SLICE_SIZE, MSM_ADDS, MSM_IMAD, RS_BYTES, MERKLE_BYTES, D2H_BYTES, \
@@ -691,9 +707,12 @@ def main():
     roofline = {
         "kernel": "k_fb_accum", "bound": "imad", "achieved": achieved, "peak": imad, "unit": "G IMAD/s",
         "frac": achieved / imad, "traffic": profile_traffic(),
-        "note": "work = 1509949440 mixed adds/blob x 10 Fq mul x 264 IMAD (reference decomposition); "
+        "note": "work = 1509949440 mixed adds/blob x 10 Fq mul x 264 IMAD (reference decomposition; "
+                f"this build executes {executed_mixed_adds(LOG_ROW, LOG_COL)} table-point additions plus "
+                "the bucket reductions, half of the products on the FP64 pipe, so frac may exceed 1); "
                 "peak = live mad.lo.u32 probe on this GPU (of measured); traffic = dram bytes per launch "
                 "from the committed ncu summary",
+        "executed_mixed_adds": executed_mixed_adds(LOG_ROW, LOG_COL),
     }
     phase_roofs = {
         "rs_extension": {"bound": "hbm", "bytes": RS_BYTES, "ms": phases["rs"],
