@@ -49,9 +49,11 @@ typedef struct zg_config {
   int device;              /* CUDA device ordinal */
   uint32_t msm_window_bits;/* 0 = auto: 11-bit fixed-base windows when the window
                               tables fit in HBM (else 8-bit), and with 1024
-                              columns 16-bit fixed-base windows for the AMT
-                              lines whose nodes hold >= 2^15 points when those
-                              tables fit too; 11 = 11-bit tables only; 8 */
+                              columns wider fixed-base windows (12 to 16 bits,
+                              one width per AMT line by its node size) for the
+                              lines whose nodes hold more than 1024 points, as
+                              far as those tables fit with 8 GiB to spare;
+                              11 = 11-bit tables only; 8 */
 } zg_config;
 
 /* Builds the device-resident encoder params (3 cosets x (LR + 2) G1 lines).
@@ -123,7 +125,7 @@ typedef struct zg_tuning {
   uint32_t ntt_threads;
   float msm_ms[3];
   float ntt_ms[9];
-  uint32_t msm_wide_lines; /* read-only: AMT lines on 16-bit windows (0 = none) */
+  uint32_t msm_wide_lines; /* read-only: AMT lines on wide windows (0 = none) */
 } zg_tuning;
 int zg_ctx_autotune(zg_ctx* ctx, zg_tuning* out);
 int zg_ctx_get_tuning(zg_ctx* ctx, zg_tuning* out);
