@@ -12,6 +12,7 @@
 #include <cstdio>
 #include <cstring>
 #include <map>
+#include <set>
 #include <mutex>
 #include <thread>
 #include <deque>
@@ -187,13 +188,14 @@ inline unsigned nblk(size_t n, unsigned t) { return (unsigned)((n + t - 1) / t);
 
 // natural-order N-point transform out = DFT(x) (or inverse without 1/N), via
 // the column / row passes; tmp has N elements
-void ntt4(const Twiddles& tw, const Fr* x, Fr* tmp, Fr* out, bool inverse, cudaStream_t s) {
+// (batch vectors back to back in x, tmp and out; batch <= 65535)
+void ntt4(const Twiddles& tw, const Fr* x, Fr* tmp, Fr* out, bool inverse, cudaStream_t s, uint32_t batch = 1) {
   const int lr = tw.lr, lc = tw.lc;
   const size_t R = size_t(1) << lr, C = size_t(1) << lc;
-  k_ntt4_colpass<<<(unsigned)C, 256, R * sizeof(Fr), s>>>(x, tmp, lr, lc, inverse ? tw.twi_r : tw.twf_r,
-                                                          inverse ? tw.wni_lo : tw.wn_lo,
-                                                          inverse ? tw.wni_hi : tw.wn_hi);
-  k_ntt4_rowpass<<<(unsigned)R, 256, C * sizeof(Fr), s>>>(tmp, out, lr, lc, inverse ? tw.twi_c : tw.twf_c);
+  k_ntt4_colpass<<<dim3((unsigned)C, batch), 256, R * sizeof(Fr), s>>>(x, tmp, lr, lc, inverse ? tw.twi_r : tw.twf_r,
+                                                                      inverse ? tw.wni_lo : tw.wn_lo,
+                                                                      inverse ? tw.wni_hi : tw.wn_hi);
+  k_ntt4_rowpass<<<dim3((unsigned)R, batch), 256, C * sizeof(Fr), s>>>(tmp, out, lr, lc, inverse ? tw.twi_c : tw.twf_c);
 }
 
 }  // namespace
@@ -883,11 +885,66 @@ const Twiddles* cached_twiddles(int lr, int lc) {
   return &(g_ntt_tw[key] = t);
 }
 
-__global__ void k_canon_to_mont(Fr* v, uint64_t total, int logn, Fr g, int coset) {
+// g^e for e < 2^logn as lo[e & (2^h - 1)] * hi[e >> h], h = (logn + 1) / 2
+// (Montgomery form), for the coset shift of zg_ntt; one pair per (logn, coset)
+struct CosetPows {
+  Fr* lo = nullptr;
+  Fr* hi = nullptr;
+  int h = 0;
+};
+std::map<std::pair<int, uint32_t>, CosetPows> g_coset_pows;  // guarded by g_ntt_mu
+
+const CosetPows* cached_coset_pows(int logn, uint32_t coset) {
+  std::lock_guard<std::mutex> g(g_ntt_mu);
+  auto key = std::make_pair(logn, coset);
+  auto it = g_coset_pows.find(key);
+  if (it != g_coset_pows.end()) return &it->second;
+  CosetPows p;
+  p.h = (logn + 1) / 2;
+  const size_t nlo = size_t(1) << p.h, nhi = size_t(1) << (logn - p.h);
+  const Fr gen = coset_factor(logn, coset);
+  std::vector<Fr> lo(nlo), hi(nhi);
+  lo[0] = Fr::one();
+  for (size_t j = 1; j < nlo; ++j) lo[j] = lo[j - 1] * gen;
+  const Fr gh = lo[nlo - 1] * gen;  // g^(2^h)
+  hi[0] = Fr::one();
+  for (size_t j = 1; j < nhi; ++j) hi[j] = hi[j - 1] * gh;
+  if (cudaMalloc(&p.lo, nlo * sizeof(Fr)) != cudaSuccess || cudaMalloc(&p.hi, nhi * sizeof(Fr)) != cudaSuccess ||
+      cudaMemcpy(p.lo, lo.data(), nlo * sizeof(Fr), cudaMemcpyHostToDevice) != cudaSuccess ||
+      cudaMemcpy(p.hi, hi.data(), nhi * sizeof(Fr), cudaMemcpyHostToDevice) != cudaSuccess) {
+    if (p.lo) cudaFree(p.lo);
+    if (p.hi) cudaFree(p.hi);
+    return nullptr;
+  }
+  return &(g_coset_pows[key] = p);
+}
+
+// The stream-ordered pool of the current device keeps freed memory instead of
+// returning it at every synchronisation, so zg_ntt's per-call scratch
+// (cudaMallocAsync / cudaFreeAsync) is mapped once, not once per call. The
+// pool then holds the largest scratch used so far (one transform batch).
+void keep_pool_memory() {
+  int dev = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess) return;
+  static std::set<int> done;  // guarded by g_ntt_mu
+  std::lock_guard<std::mutex> g(g_ntt_mu);
+  if (!done.insert(dev).second) return;
+  cudaMemPool_t pool;
+  if (cudaDeviceGetDefaultMemPool(&pool, dev) != cudaSuccess) return;
+  uint64_t keep = UINT64_MAX;
+  cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &keep);
+}
+
+// canonical -> Montgomery, times g^(i mod 2^logn) when lo is set
+__global__ void k_canon_to_mont(Fr* v, uint64_t total, int logn, const Fr* __restrict__ lo, const Fr* __restrict__ hi,
+                                int h) {
   uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= total) return;
   Fr x = Fr::from_canonical(v[i]);
-  if (coset) x = x * g.pow_u64(i & ((1ull << logn) - 1));
+  if (lo) {
+    const uint32_t e = (uint32_t)(i & ((1ull << logn) - 1));
+    x = x * (lo[e & ((1u << h) - 1)] * hi[e >> h]);
+  }
   v[i] = x;
 }
 __global__ void k_mont_to_canon(Fr* v, uint64_t n, Fr scale, int do_scale) {
@@ -2156,6 +2213,7 @@ int zg_verify_slices(zg_ctx* c, const uint8_t* const* slices, const size_t* lens
   if (!c->fb) return fail(ZG_ERR_INVALID_ARG, "zg_verify_slices needs the fixed-base tables (msm_window_bits 0 or 11)");
   std::lock_guard<std::mutex> g(c->mu);
   ZG_CK(cudaSetDevice(c->device));
+  keep_pool_memory();
   int rc = ensure_g2(c);
   if (rc) return rc;
   const uint64_t R = c->R, C = c->C;
@@ -2416,6 +2474,7 @@ int zg_msm_chunks(const void* d_bases, const void* d_scalars, uint32_t lines, ui
   const size_t nch = size_t(1) << log_nchunks;
   const size_t count = (size_t)lines * nch;
   XYZZ *win = nullptr, *part = nullptr;
+  keep_pool_memory();
   ZG_CK(cudaMallocAsync(&win, count * MSM_WINDOWS * sizeof(XYZZ), s));
   ZG_CK(cudaMallocAsync(&part, count * sizeof(XYZZ), s));
   MsmChunkArgs a;
@@ -2718,10 +2777,12 @@ int zg_ntt(void* d_data, uint32_t log_n, uint32_t batch, int inverse, uint32_t c
   const size_t n = size_t(1) << log_n;
   Fr* v = (Fr*)d_data;
   const unsigned T = 256;
-  Fr g = coset_idx ? coset_factor((int)log_n, coset_idx) : Fr::one();
+  const CosetPows* cp = nullptr;
+  if (coset_idx && !(cp = cached_coset_pows((int)log_n, coset_idx))) return fail(ZG_ERR_CUDA, "coset table alloc failed");
   Fr ninv = host_fr_from_u32((uint32_t)n).inverse();
   const uint64_t total = (uint64_t)batch * n;
-  k_canon_to_mont<<<nblk(total, T), T, 0, s>>>(v, total, (int)log_n, g, coset_idx ? 1 : 0);
+  k_canon_to_mont<<<nblk(total, T), T, 0, s>>>(v, total, (int)log_n, cp ? cp->lo : nullptr, cp ? cp->hi : nullptr,
+                                               cp ? cp->h : 0);
   if (log_n <= 11) {
     const Twiddles* tw = cached_twiddles(0, (int)log_n);
     if (!tw) return ZG_ERR_CUDA;
@@ -2734,9 +2795,14 @@ int zg_ntt(void* d_data, uint32_t log_n, uint32_t batch, int inverse, uint32_t c
     const int lc = (int)(log_n + 1) / 2, lr = (int)log_n - lc;
     const Twiddles* tw = cached_twiddles(lr, lc);
     if (!tw) return ZG_ERR_CUDA;
+    const uint32_t per = std::min<uint32_t>(batch, 65535);
+    keep_pool_memory();
     Fr* tmp = nullptr;
-    ZG_CK(cudaMallocAsync(&tmp, n * sizeof(Fr), s));
-    for (uint32_t b = 0; b < batch; ++b) ntt4(*tw, v + (size_t)b * n, tmp, v + (size_t)b * n, inverse != 0, s);
+    ZG_CK(cudaMallocAsync(&tmp, (size_t)per * n * sizeof(Fr), s));
+    for (uint32_t b0 = 0; b0 < batch; b0 += per) {
+      const uint32_t nb = std::min<uint32_t>(batch - b0, per);
+      ntt4(*tw, v + (size_t)b0 * n, tmp, v + (size_t)b0 * n, inverse != 0, s, nb);
+    }
     cudaFreeAsync(tmp, s);
   }
   k_mont_to_canon<<<nblk(total, T), T, 0, s>>>(v, total, ninv, inverse ? 1 : 0);
@@ -2842,6 +2908,7 @@ int zg_merkle_roots(const void* d_items, size_t n_items, void* d_roots, void* st
   }
   cudaStream_t s = (cudaStream_t)stream;
   uint8_t* tree = nullptr;
+  keep_pool_memory();
   ZG_CK(cudaMallocAsync(&tree, o, s));
   int rc = merkle_levels((const uint8_t*)d_items, n_items, tree, off, depth, s);
   if (!rc) ZG_CK(cudaMemcpyAsync(d_roots, tree, 96, cudaMemcpyDeviceToDevice, s));

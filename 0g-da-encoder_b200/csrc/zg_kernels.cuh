@@ -1196,6 +1196,7 @@ __global__ void k_quot_coeff(const Fr* pw, Fr* c, uint32_t M, uint32_t n) {
 
 // generic four-step NTT pass A: for each column s (C of them) of x viewed as
 // [R][C] row-major: R-point transform over q, times w_N^{s r}; writes Y[r][s].
+// blockIdx.y selects the vector of a batch (vectors of R C elements back to back).
 __global__ void __launch_bounds__(256) k_ntt4_colpass(const Fr* __restrict__ x, Fr* __restrict__ y, int lr, int lc,
                                const Fr* __restrict__ tw_r, const Fr* __restrict__ w_lo,
                                const Fr* __restrict__ w_hi) {
@@ -1203,6 +1204,8 @@ __global__ void __launch_bounds__(256) k_ntt4_colpass(const Fr* __restrict__ x, 
   const int R = 1 << lr, C = 1 << lc;
   Fr* s = reinterpret_cast<Fr*>(smem);
   const uint32_t col = blockIdx.x;
+  x += (size_t)blockIdx.y << (lr + lc);
+  y += (size_t)blockIdx.y << (lr + lc);
   for (int q = threadIdx.x; q < R; q += blockDim.x) s[brev_bits(q, lr)] = load_fr(x + (size_t)q * C + col);
   __syncthreads();
   ntt_smem(s, lr, tw_r);
@@ -1217,6 +1220,8 @@ __global__ void __launch_bounds__(256) k_ntt4_rowpass(const Fr* __restrict__ y, 
   const int R = 1 << lr, C = 1 << lc;
   Fr* s = reinterpret_cast<Fr*>(smem);
   const uint32_t r = blockIdx.x;
+  y += (size_t)blockIdx.y << (lr + lc);
+  out += (size_t)blockIdx.y << (lr + lc);
   for (int k = threadIdx.x; k < C; k += blockDim.x) s[brev_bits(k, lc)] = load_fr(y + (size_t)r * C + k);
   __syncthreads();
   ntt_smem(s, lc, tw_c);

@@ -73,6 +73,7 @@ def test_device_arithmetic_selftest(gpu_pkg):
 @pytest.mark.parametrize("log_n,batch,inverse,coset", [
     (5, 4, 0, 0), (5, 4, 1, 0), (5, 3, 0, 1), (10, 8, 0, 0), (10, 8, 1, 0), (10, 2, 0, 2),
     (11, 2, 1, 0), (14, 1, 0, 0), (14, 1, 1, 0), (20, 1, 0, 1), (20, 1, 1, 0),
+    (12, 4, 0, 1), (13, 3, 1, 0), (14, 5, 0, 2),  # batched four-step passes
 ])
 def test_ntt_matches_oracle(gpu_pkg, oracle, log_n, batch, inverse, coset):
     rng = np.random.default_rng(log_n * 100 + batch + inverse)
