@@ -2644,15 +2644,22 @@ int zg_ctx_msm(zg_ctx* c, uint32_t coset, uint32_t line, const void* d_scalars, 
   if (!c->fb) return fail(ZG_ERR_INVALID_ARG, "zg_ctx_msm needs the fixed-base tables (msm_window_bits 0 or 11)");
   if (coset >= 3 || line >= (uint32_t)c->L) return fail(ZG_ERR_INVALID_ARG, "coset or line out of range");
   if (n < c->C || n > c->N || (n & (n - 1))) return fail(ZG_ERR_INVALID_ARG, "n must be a power of two in [2^log_col, N]");
-  int lrn = 0;
-  while (((size_t)c->C << lrn) < n) ++lrn;
+  // work items = chunks of 2^lcs points: 1024-point chunks leave most SMs
+  // idle below 2^19 points (one CTA per item), so chunks shrink down to 128
+  // points until there are 512 items, as far as the context's chunk buffers
+  // (3 R chunks) allow; the tables are per point, so any chunking reads them
+  int logn = 0;
+  while (((size_t)1 << logn) < n) ++logn;
+  int lcs = c->lc;
+  while (lcs > 7 && (n >> lcs) < 512 && (n >> (lcs - 1)) <= 3 * c->R) --lcs;
+  const int lrn = logn - lcs;
   const uint32_t nch = 1u << lrn;
   std::lock_guard<std::mutex> g(c->mu);
   ZG_CK(cudaSetDevice(c->device));
   cudaStream_t s = (cudaStream_t)stream;
   ZG_CK(cudaStreamWaitEvent(s, c->done, 0));
-  k_fb_sort<<<dim3(nch, 1), 256, fb_sort_smem_bytes(c->lc), s>>>((const uint8_t*)d_scalars, c->fb_offs, c->fb_ents,
-                                                                  lrn, c->lc, 0, 0);
+  k_fb_sort<<<dim3(nch, 1), 256, fb_sort_smem_bytes(lcs), s>>>((const uint8_t*)d_scalars, c->fb_offs, c->fb_ents,
+                                                                lrn, lcs, 0, 0);
   FbAccArgs fa;
   fa.tab = c->line_ptr((int)coset, (int)line);
   fa.offs = c->fb_offs;
@@ -2661,7 +2668,7 @@ int zg_ctx_msm(zg_ctx* c, uint32_t coset, uint32_t line, const void* d_scalars, 
   fa.outS = c->fb_S;
   fa.ents32 = nullptr;
   fa.lr = lrn;
-  fa.lc = c->lc;
+  fa.lc = lcs;
   fa.lines = 1;
   fa.l0 = 0;
   fa.Ltot = 1;

@@ -165,6 +165,32 @@ def test_ctx_msm_rejects_bad_sizes(gpu_pkg, ctx_4x6):
         assert L.zg_ctx_msm(ctx_4x6.handle, coset, line, ts.data_ptr(), n, out.data_ptr(), None) != 0
 
 
+@pytest.fixture(scope="module")
+def ctx_5x10(gpu_pkg):
+    params = gpu_pkg.ZgEncoderParams.from_seed(5, 10, 9)
+    yield params
+    params.close()
+
+
+@pytest.mark.parametrize("n,coset,line", [(1 << 11, 0, 6), (1 << 13, 1, 0), (1 << 15, 2, 5)])
+def test_ctx_msm_small_chunks_match_oracle(gpu_pkg, oracle, ctx_5x10, n, coset, line):
+    """On a 1024-column context zg_ctx_msm cuts MSMs that would give few
+    1024-point chunks into smaller chunks (here 128 points for 2^11 and 2^13
+    points, 512 for 2^15, capped by the context's chunk buffers); the result
+    is the oracle's Pippenger on the same points."""
+    rng = np.random.default_rng(n + coset)
+    scal = bytearray(rand_fr_bytes(rng, n))
+    for i, v in enumerate([0, 1, R_MOD - 1, 2, 1 << 252]):
+        scal[32 * i:32 * i + 32] = v.to_bytes(32, "little")
+    scal = bytes(scal)
+    bases = ctx_5x10.param_line(coset, line, 0, n)
+    out = empty(64)
+    ts = dev(scal)
+    rc = gpu_pkg.lib().zg_ctx_msm(ctx_5x10.handle, coset, line, ts.data_ptr(), n, out.data_ptr(), None)
+    assert rc == 0, gpu_pkg.lib().zg_last_error()
+    assert host(out) == oracle.msm(bases, scal)
+
+
 def test_msm_special_cases(gpu_pkg, oracle, small_params_mont):
     """Doubling and cancellation inside buckets: repeated and negated bases."""
     line = mont_lines(small_params_mont[0], 4, 6)[0]
