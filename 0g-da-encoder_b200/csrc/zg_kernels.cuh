@@ -673,7 +673,7 @@ struct FbAccPlan {
   uint32_t start[FB_MAX_SETS + 1] = {};
   FbAccArgs a[FB_MAX_SETS];
 };
-constexpr int FB_TASK = 32;
+constexpr int FB_TASK = 64;
 constexpr int FB_MAX_TASKS = FB_BUCKETS + FB_WINDOWS * 1024 / FB_TASK;  // chunk <= 1024 points
 // M is the product kind of the point additions (MulImad / MulHybrid / MulF64,
 // chosen by the context's tuning; identical results).
