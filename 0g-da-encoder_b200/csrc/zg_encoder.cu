@@ -13,6 +13,7 @@
 #include <cstring>
 #include <map>
 #include <set>
+#include <tuple>
 #include <mutex>
 #include <thread>
 #include <deque>
@@ -873,11 +874,19 @@ int encode_device_locked(zg_ctx* c, const uint8_t* d_data, size_t len, cudaStrea
 }
 
 std::mutex g_ntt_mu;
-std::map<std::pair<int, int>, Twiddles> g_ntt_tw;
+// twiddle tables of the standalone entry points, per (device, lr, lc): device
+// memory of the device current at the call
+std::map<std::tuple<int, int, int>, Twiddles> g_ntt_tw;
+
+int current_device() {
+  int dev = 0;
+  cudaGetDevice(&dev);
+  return dev;
+}
 
 const Twiddles* cached_twiddles(int lr, int lc) {
   std::lock_guard<std::mutex> g(g_ntt_mu);
-  auto key = std::make_pair(lr, lc);
+  auto key = std::make_tuple(current_device(), lr, lc);
   auto it = g_ntt_tw.find(key);
   if (it != g_ntt_tw.end()) return &it->second;
   Twiddles t;
@@ -886,17 +895,18 @@ const Twiddles* cached_twiddles(int lr, int lc) {
 }
 
 // g^e for e < 2^logn as lo[e & (2^h - 1)] * hi[e >> h], h = (logn + 1) / 2
-// (Montgomery form), for the coset shift of zg_ntt; one pair per (logn, coset)
+// (Montgomery form), for the coset shift of zg_ntt; one pair per (device, logn,
+// coset)
 struct CosetPows {
   Fr* lo = nullptr;
   Fr* hi = nullptr;
   int h = 0;
 };
-std::map<std::pair<int, uint32_t>, CosetPows> g_coset_pows;  // guarded by g_ntt_mu
+std::map<std::tuple<int, int, uint32_t>, CosetPows> g_coset_pows;  // per device; guarded by g_ntt_mu
 
 const CosetPows* cached_coset_pows(int logn, uint32_t coset) {
   std::lock_guard<std::mutex> g(g_ntt_mu);
-  auto key = std::make_pair(logn, coset);
+  auto key = std::make_tuple(current_device(), logn, coset);
   auto it = g_coset_pows.find(key);
   if (it != g_coset_pows.end()) return &it->second;
   CosetPows p;
