@@ -362,6 +362,9 @@ constexpr int FB_WINDOWS = 24;                    // ceil((254 + 1) / 11)
 constexpr int FB_BUCKETS = 1 << (FB_BITS - 1);    // 1024
 constexpr int FB_ACC_THREADS = 128;
 constexpr int FB_PER_THREAD = FB_BUCKETS / FB_ACC_THREADS;  // 8 buckets per thread
+__host__ __device__ constexpr int fb_log2(int x) { return x <= 1 ? 0 : 1 + fb_log2(x / 2); }
+constexpr int FB_PER_THREAD_LOG = fb_log2(FB_PER_THREAD);
+constexpr int FB_ACC_MIN_CTAS = 512 / FB_ACC_THREADS;  // resident CTAs per SM at 128 registers
 
 // Wide windows for the AMT lines whose nodes are MSMs over more than 1024
 // points. Such a line's nodes are cut into sort units of U = 2^ulog points
@@ -678,7 +681,7 @@ constexpr int FB_MAX_TASKS = FB_BUCKETS + FB_WINDOWS * 1024 / FB_TASK;  // chunk
 // M is the product kind of the point additions (MulImad / MulHybrid / MulF64,
 // chosen by the context's tuning; identical results).
 template <class M>
-__global__ void __launch_bounds__(FB_ACC_THREADS, 4) k_fb_accum(const FbAccPlan plan, XYZZ* __restrict__ gpart_all,
+__global__ void __launch_bounds__(FB_ACC_THREADS, FB_ACC_MIN_CTAS) k_fb_accum(const FbAccPlan plan, XYZZ* __restrict__ gpart_all,
                                                                 uint32_t* __restrict__ next) {
   __shared__ uint32_t soffs[FB_BUCKETS + 1];
   __shared__ uint16_t tstart[FB_BUCKETS + 1];
@@ -882,7 +885,7 @@ __global__ void __launch_bounds__(64) k_fb_combine(const XYZZ* __restrict__ T, c
   }
   for (int i = 0; i < FB_ACC_THREADS; ++i) tot.add(load_xyzz(t + i));
 #pragma unroll 1
-  for (int k = 0; k < 3; ++k) wsum = wsum.dbl();  // x FB_PER_THREAD = 8
+  for (int k = 0; k < FB_PER_THREAD_LOG; ++k) wsum = wsum.dbl();  // x FB_PER_THREAD
   tot.add(wsum);
   const uint32_t blk = fb_item_block(m, v);
   if (blk) {
@@ -906,25 +909,27 @@ __device__ __forceinline__ XYZZ shfl_xor_xyzz(const XYZZ& p, int m) {
 
 // k_fb_combine with one warp per item, for launches with few items (the
 // single MSMs of zg_ctx_msm and of slice verification: 1024 items leave
-// k_fb_combine's one thread per item on a handful of SMs). Lane l folds
-// partials 4l .. 4l+3 into t_l, s_l and w_l = sum_k k S_{4l+k}; then
-// sum_i i S_i = 4 sum_l l s_l + sum_l w_l, sum_l l s_l being the sum over
+// k_fb_combine's one thread per item on a handful of SMs). With P =
+// FB_ACC_THREADS / 32 partials per lane, lane l folds partials P l .. P l +
+// P - 1 into t_l, s_l and w_l = sum_k k S_{Pl+k}; then
+// sum_i i S_i = P sum_l l s_l + sum_l w_l, sum_l l s_l being the sum over
 // lanes l >= 1 of the suffix sums U_l = sum_{m >= l} s_m (a warp scan). About
 // three times the additions of k_fb_combine, so blob encodes keep that one.
 __global__ void __launch_bounds__(128) k_fb_combine_warp(const XYZZ* __restrict__ T, const XYZZ* __restrict__ S,
                                                          XYZZ* __restrict__ part, FbCombinePlan plan) {
-  static_assert(FB_ACC_THREADS == 128, "four partials per lane");
+  constexpr int P = FB_ACC_THREADS / 32;  // partials per lane
+  static_assert(P >= 1 && (P & (P - 1)) == 0, "a power of two of partials per lane");
   const uint32_t u = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   const int lane = threadIdx.x & 31;
   if (u >= plan.start[plan.n]) return;  // uniform per warp
   uint32_t v;
   const FbCombineMap& m = fb_plan_item(plan, u, &v);
-  const XYZZ* t = T + (size_t)u * FB_ACC_THREADS + 4 * lane;
-  const XYZZ* s = S + (size_t)u * FB_ACC_THREADS + 4 * lane;
+  const XYZZ* t = T + (size_t)u * FB_ACC_THREADS + P * lane;
+  const XYZZ* s = S + (size_t)u * FB_ACC_THREADS + P * lane;
   XYZZ tl = load_xyzz(t);
-  for (int k = 1; k < 4; ++k) tl.add(load_xyzz(t + k));
-  XYZZ run = load_xyzz(s + 3), w = run;
-  for (int k = 2; k >= 1; --k) {
+  for (int k = 1; k < P; ++k) tl.add(load_xyzz(t + k));
+  XYZZ run = XYZZ::inf(), w = XYZZ::inf();
+  for (int k = P - 1; k >= 1; --k) {
     run.add(load_xyzz(s + k));
     w.add(run);
   }
@@ -941,9 +946,11 @@ __global__ void __launch_bounds__(128) k_fb_combine_warp(const XYZZ* __restrict_
     a.add(shfl_xor_xyzz(a, mk));
   }
   if (lane == 0) {
-    a = a.dbl().dbl();        // 4 sum_l l s_l
-    a.add(w);                 // sum_i i S_i
-    a = a.dbl().dbl().dbl();  // x FB_PER_THREAD = 8
+#pragma unroll 1
+    for (int k = 0; k < fb_log2(P); ++k) a = a.dbl();  // P sum_l l s_l
+    a.add(w);                                           // sum_i i S_i
+#pragma unroll 1
+    for (int k = 0; k < FB_PER_THREAD_LOG; ++k) a = a.dbl();  // x FB_PER_THREAD
     tl.add(a);
     const uint32_t blk = fb_item_block(m, v);
     if (blk) tl.add(fb_block_term(U, blk));  // U at lane 0 = sum of all the item's buckets
