@@ -7,7 +7,7 @@ include/zg_encoder.h (ctypes):
   -------------------------------------------------  ---------------------------
   constants BLOB_ROW_LOG/BLOB_COL_LOG/...             Dims
   (crates/encoder/src/constants.rs:14-28)
-  RawData::try_from(&[u8]) (raw_data.rs:76-95)        RawData.try_from(bytes)
+  RawData::try_from(&[u8]) (raw_data.rs:55-72)        RawData.try_from(bytes)
   EncoderError::TooLargeBlob (encoder/error.rs:3-6)   TooLargeBlob
   ZgEncoderParams::from_dir_mont (blob/encode.rs:114) ZgEncoderParams.from_dir_mont
   PowerTau::setup_inner(Some(tau)) + from_pp          ZgEncoderParams.from_seed
@@ -247,7 +247,7 @@ class TooLargeBlob(EncoderError):
 
 class RawData:
     """RawData: payload zero-padded to MAX_BLOB_SIZE with its LE u32 length in
-    the last four bytes (crates/encoder/src/raw_data.rs:8-95)."""
+    the last four bytes (crates/encoder/src/raw_data.rs:8-72)."""
 
     def __init__(self, padded: bytes, dims: Dims):
         self.padded = padded
@@ -488,7 +488,9 @@ def verify_slices(params: ZgEncoderParams, slices, commitment: bytes, storage_ro
     """EncodedSlice::verify (crates/encoder/src/encoder/slice.rs:73-95) for a
     batch of serialized slices of one blob, on the GPU (zg_verify_slices).
     Returns (codes, details): per slice the verdict code and its 4 detail
-    fields [AmtProofError, a, b, c]."""
+    fields [AmtProofError, a, b, c]. seed=0 draws the batch coefficients from
+    the OS CSPRNG; a nonzero seed makes them reproducible, for tests only (a
+    party that knows the seed can craft slices that pass)."""
     n = len(slices)
     ptrs = (ctypes.c_char_p * max(n, 1))(*slices)
     lens = (ctypes.c_size_t * max(n, 1))(*[len(x) for x in slices])

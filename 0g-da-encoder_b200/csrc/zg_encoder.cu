@@ -7,6 +7,8 @@
 // serialised by a mutex; use one context per stream of work for overlap.
 #include <cuda_runtime.h>
 #include <dirent.h>
+#include <errno.h>
+#include <sys/random.h>
 
 #include <condition_variable>
 #include <cstdio>
@@ -163,11 +165,16 @@ size_t msm_smem_bytes(int lc) {
   return C * 32 + (size_t)MSM_WINDOWS * C * 2 + MSM_WINDOWS * 129 * 2 + 129 * 4 + 16;
 }
 
+// The dynamic shared-memory limit is a per-device attribute of each kernel,
+// so it is raised once for every device a call runs on (the device current at
+// the call).
 int set_smem_limits() {
-  static bool done = false;
+  static std::set<int> done;
   static std::mutex m;
   std::lock_guard<std::mutex> g(m);
-  if (done) return 0;
+  int dev = 0;
+  ZG_CK(cudaGetDevice(&dev));
+  if (done.count(dev)) return 0;
   const int big = 227 * 1024;
   ZG_CK(cudaFuncSetAttribute(k_rows_from_raw, cudaFuncAttributeMaxDynamicSharedMemorySize, big));
   ZG_CK(cudaFuncSetAttribute(k_cols, cudaFuncAttributeMaxDynamicSharedMemorySize, big));
@@ -181,7 +188,7 @@ int set_smem_limits() {
   ZG_CK(cudaFuncSetAttribute(k_wd_sort<11>, cudaFuncAttributeMaxDynamicSharedMemorySize, big));
   ZG_CK(cudaFuncSetAttribute(k_ntt4_colpass, cudaFuncAttributeMaxDynamicSharedMemorySize, big));
   ZG_CK(cudaFuncSetAttribute(k_ntt4_rowpass, cudaFuncAttributeMaxDynamicSharedMemorySize, big));
-  done = true;
+  done.insert(dev);
   return 0;
 }
 
@@ -1547,10 +1554,33 @@ bool parse_slice(const uint8_t* in, size_t len, PSlice* s) {
   return p == end;
 }
 
-// SplitMix64 stream of 128-bit coefficients (below r)
+// 128-bit coefficients (below r) of the random linear combinations. With
+// os set, every coefficient is drawn from the kernel's CSPRNG (getrandom), so
+// a batch that fails the checks passes a combination with probability at
+// most 2^-128 (a nonzero degree-1 polynomial in a uniform 128-bit
+// coefficient vanishes for at most one value of it). Otherwise they come from
+// a SplitMix64 stream at a caller-given seed: reproducible, for tests, and
+// not safe against slices built by someone who knows the seed.
 struct Coeffs {
-  uint64_t s;
+  uint64_t s = 0;
+  bool os = false;
+  bool failed = false;  // the OS generator did not answer
   void next(uint32_t w[4]) {
+    if (os) {
+      uint8_t* p = reinterpret_cast<uint8_t*>(w);
+      size_t got = 0;
+      while (got < 16) {
+        const ssize_t k = getrandom(p + got, 16 - got, 0);
+        if (k < 0) {
+          if (errno == EINTR) continue;
+          failed = true;
+          memset(w, 0, 16);
+          return;
+        }
+        got += (size_t)k;
+      }
+      return;
+    }
     for (int k = 0; k < 2; ++k) {
       const uint64_t x = splitmix64(s);
       w[2 * k] = (uint32_t)x;
@@ -1644,6 +1674,7 @@ int amt_batch(VerifyRun& v, const std::vector<uint32_t>& ids, bool* ok) {
     for (int d = 0; d < LR; ++d) v.rng.next(&beta_w[4 * (j * LR + d)]);
     v.rng.next(&gamma_w[4 * j]);
   }
+  if (v.rng.failed) return fail(ZG_ERR_INTERNAL, "getrandom failed: no coefficients for the batch checks");
   // MSM check scalars
   bool present[3] = {false, false, false};
   std::vector<uint32_t> h_pos(n), h_cos(n), h_bi(n);
@@ -1995,7 +2026,7 @@ int zg_encode_device(zg_ctx* c, const void* d_data, size_t len, void* stream, zg
 int zg_encode(zg_ctx* c, const uint8_t* data, size_t len, int require_data, zg_reply** out) {
   if (!c || !out || (!data && len)) return fail(ZG_ERR_INVALID_ARG, "null argument");
   *out = nullptr;
-  if (len > c->max_raw) {  // RawData::try_from (crates/encoder/src/raw_data.rs:76-95)
+  if (len > c->max_raw) {  // RawData::try_from (crates/encoder/src/raw_data.rs:55-72)
     char m[128];
     snprintf(m, sizeof(m), "TooLargeBlob { actual: %zu, expected_max: %zu }", len, c->max_raw);
     return fail(ZG_ERR_TOO_LARGE_BLOB, m);
@@ -2062,7 +2093,7 @@ int zg_submit(zg_ctx* c, const zg_request* req, uint64_t* ticket) {
   if (!c || !req || !ticket) return fail(ZG_ERR_INVALID_ARG, "null argument");
   if (req->kind == ZG_REQ_ENCODE) {
     if (!req->data && req->len) return fail(ZG_ERR_INVALID_ARG, "null payload");
-    if (req->len > c->max_raw) {  // RawData::try_from (crates/encoder/src/raw_data.rs:76-95)
+    if (req->len > c->max_raw) {  // RawData::try_from (crates/encoder/src/raw_data.rs:55-72)
       char m[128];
       snprintf(m, sizeof(m), "TooLargeBlob { actual: %zu, expected_max: %zu }", req->len, c->max_raw);
       return fail(ZG_ERR_TOO_LARGE_BLOB, m);
@@ -2234,11 +2265,8 @@ int zg_verify_slices(zg_ctx* c, const uint8_t* const* slices, const size_t* lens
   v.c = c;
   v.s = c->stream;
   v.sl = &sl;
-  if (!seed) {
-    std::random_device rd;
-    seed = ((uint64_t)rd() << 32) ^ rd();
-  }
   v.rng.s = seed;
+  v.rng.os = seed == 0;
   const bool auth_ok = g1_from_reply(commitment, &v.auth);
   // deserialization and the structural checks, in the reference's order
   // (EncodedSlice::verify, encoder/slice.rs:73-95; EncodedSliceAMT::verify,
@@ -2510,12 +2538,13 @@ int zg_msm_chunks(const void* d_bases, const void* d_scalars, uint32_t lines, ui
 // Allocation-free twin of zg_msm_chunks: same kernels, with the scratch in
 // g_noalloc_scratch. Host code must not hand the array's name to a kernel (on
 // the host it names a stand-in, not device memory), so its device address is
-// looked up with cudaGetSymbolAddress once per device, with that device
-// current, on the first call made on it; later calls reuse the cached address.
+// looked up with cudaGetSymbolAddress, with the call's device current, on
+// every call: the lookup is cheap once the module is loaded, and an address
+// cached across a cudaDeviceReset would point into the freed old module. The
+// first call on a device loads the module there and should come before any
+// stream capture.
 int zg_msm_chunks_noalloc(const void* d_bases, const void* d_scalars, uint32_t lines, uint32_t log_nchunks,
                           uint32_t log_chunk, void* d_out, void* stream) {
-  static std::mutex mu;
-  static void* addr[256] = {nullptr};
   if (!d_bases || !d_scalars || !d_out || lines == 0 || log_chunk > 10 || log_nchunks > 20)
     return fail(ZG_ERR_INVALID_ARG, "bad msm arguments");
   const uint64_t count = (uint64_t)lines << log_nchunks;
@@ -2525,21 +2554,10 @@ int zg_msm_chunks_noalloc(const void* d_bases, const void* d_scalars, uint32_t l
              (unsigned long long)count, ZG_NOALLOC_MAX_MSMS);
     return fail(ZG_ERR_INVALID_ARG, m);
   }
-  int dev = 0;
-  ZG_CK(cudaGetDevice(&dev));
-  if (dev < 0 || dev >= 256) return fail(ZG_ERR_INVALID_ARG, "device ordinal out of range");
   void* scratch = nullptr;
-  {
-    std::lock_guard<std::mutex> g(mu);
-    if (!addr[dev]) {
-      cudaError_t e = cudaGetSymbolAddress(&addr[dev], g_noalloc_scratch);
-      if (e != cudaSuccess) {
-        addr[dev] = nullptr;
-        return fail(ZG_ERR_CUDA, std::string("cudaGetSymbolAddress(g_noalloc_scratch): ") + cudaGetErrorString(e));
-      }
-    }
-    scratch = addr[dev];
-  }
+  const cudaError_t e = cudaGetSymbolAddress(&scratch, g_noalloc_scratch);
+  if (e != cudaSuccess || !scratch)
+    return fail(ZG_ERR_CUDA, std::string("cudaGetSymbolAddress(g_noalloc_scratch): ") + cudaGetErrorString(e));
   int rc = set_smem_limits();
   if (rc) return rc;
   cudaStream_t s = (cudaStream_t)stream;

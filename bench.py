@@ -23,9 +23,15 @@ tau), keccak Merkle tree, and the 3072 serialized EncodedSlices.
           rows, each result checked) through the pipeline: completed
           requests/s and p50 / p99 latency from arrival to result
 
+  cpu_baseline : one full blob of the C++ restatement of the reference CPU
+          path (oracle/, all host threads, the reference's prove.rs
+          decomposition and ark-ec's signed-digit MSM), on the same payload;
+          its file root is checked against the GPU's
+
 Multi-GPU: one process per GPU, independent replicas (weak scaling), max of
-the per-rank times. `--impl reference` times the CPU restatement of the
-reference path (the reference itself is Rust and cannot be built here).
+the per-rank times. `--impl reference` times the same CPU restatement on full
+blobs, one coset per step (three steps make one blob; the reference itself is
+Rust and cannot be built here).
 """
 import argparse
 import ctypes
@@ -51,7 +57,7 @@ R = 1 << LOG_ROW
 N = 1 << (LOG_ROW + LOG_COL)
 PAYLOAD = 31 * N - 4                      # MAX_RAW_DATA_SIZE
 SLICE_SIZE = 312 + 32 * (1 << LOG_COL) + 160 * LOG_ROW
-# algorithmic work per blob (reference decomposition)
+# algorithmic work per blob: the reference GPU-plugin decomposition (36 864 chunk MSMs of 1024 points)
 MSM_ADDS = 36864 * 40960                  # 36 864 MSMs x 1024 pts, signed 8-bit windows
 MSM_IMAD = MSM_ADDS * 10 * 264            # 10 Fq mul per mixed add, 264 32-bit IMAD per Fq mul
 RS_BYTES = 201_326_592                    # 3 transforms x (read + write 32 MiB)
@@ -116,7 +122,6 @@ def parse():
     ap.add_argument("--steps", type=int, default=5)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
-    ap.add_argument("--cpu-sample", type=int, default=0, help="chunk groups in the CPU sample (0 = auto)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--batch-blobs", type=int, default=8, help="blobs in the batched-uneven sample")
     ap.add_argument("--serve-rate", default="2,8",
@@ -252,54 +257,63 @@ def dist_setup():
     return rank, world, local
 
 
-def cpu_sample_chunks(S):
-    rng = np.random.default_rng(7)
-    return sorted(rng.choice(3 * R, size=S, replace=False).tolist())
+CPU_SAMPLE = ("full 1024x1024 blobs of the C++ restatement of the reference CPU path (oracle/), one coset per "
+              "step, 3 steps = 1 blob: RawData -> RawBlob -> 3-coset RS extension (to_coset_blob, ark-poly style "
+              "radix-2), AMT commitment + proofs with the reference CPU decomposition (prove.rs:58-102: layer d = "
+              "2^d MSMs of 2^(20-d) points, 1024 x 1024 commitment tree, one 2^20 high MSM; each MSM ark-ec's "
+              "signed-digit bucket method, windows in parallel), keccak Merkle tree, 3072 serialized slices; "
+              "params of the seeded tau built on the CPU; nothing sampled or scaled (the Rust reference cannot "
+              "be built here)")
 
 
-def cpu_baseline_run(payload, sample_bases, chunks):
+def cpu_blob_steps(o, params, payload, warmup, steps):
+    """Times `steps` coset steps of the restated CPU path after `warmup`
+    untimed ones, starting each timed run on a blob boundary. Returns
+    (blobs/s, total seconds, per-step seconds, file root of the last blob)."""
+    job = o.cpu_job(params, payload)
+    done = 0
+    root = None
+    while done < warmup or done % 3:
+        _, r, _ = job.step()
+        root = r or root
+        done += 1
+    times = []
+    for _ in range(steps):
+        t0 = time.perf_counter()
+        _, r, _ = job.step()
+        times.append(time.perf_counter() - t0)
+        root = r or root
+    total = sum(times)
+    return (steps / 3.0) / total, total, times, root
+
+
+def cpu_oracle():
     sys.path.insert(0, os.path.join(ROOT, "tests"))
     import zgo
-    o = zgo.Oracle()
-    t_rs, t_merkle, t_msm = o.cpu_baseline(LOG_ROW, LOG_COL, payload, sample_bases, chunks)
-    S = len(chunks)
-    per_blob = t_rs + t_merkle + t_msm * (3 * R) / S
-    cores = o.L.zgo_num_threads()
-    return 1.0 / per_blob, cores, {"rs_s": t_rs, "merkle_s": t_merkle, "msm_sample_s": t_msm, "per_blob_s": per_blob}
-
-
-def auto_sample():
-    cores = os.cpu_count() or 8
-    return int(max(16, min(3 * R, 8 * cores)))
+    return zgo.Oracle()
 
 
 def reference_arm(args, rank):
-    """CPU restatement of the reference path (oracle/), all host threads."""
+    """The reference's CPU path (its C++ restatement, oracle/) on all host
+    threads, full blobs, one coset per step."""
     if rank != 0:
         return
-    sys.path.insert(0, os.path.join(ROOT, "tests"))
-    import zgo
-    o = zgo.Oracle()
-    S = args.cpu_sample or max(8, auto_sample() // 4)
-    chunks = cpu_sample_chunks(S)
+    o = cpu_oracle()
+    t0 = time.perf_counter()
+    params = o.params(LOG_ROW, LOG_COL, PARAM_SEED)
+    t_params = time.perf_counter() - t0
     payload = np.random.default_rng(DATA_SEED).integers(0, 256, size=PAYLOAD, dtype=np.uint8).tobytes()
-    L = LOG_ROW + 2
-    bases = o.random_points(99, S * L * (1 << LOG_COL))
-    vals = []
-    for step in range(args.warmup + args.steps):
-        v, cores, detail = cpu_baseline_run(payload, bases, chunks)
-        if step >= args.warmup:
-            vals.append(v)
-    value = statistics.mean(vals)
-    sample = (f"per step: full RS extension + Merkle on 1 blob, MSM work sampled as {S} of 3072 chunk groups "
-              f"(12 line-MSMs of 1024 points each, stand-in points of G1) scaled by 3072/{S}; "
-              f"C++ restatement of the reference CPU path (the Rust reference cannot be built here)")
+    value, total, times, _ = cpu_blob_steps(o, params, payload, args.warmup, args.steps)
+    cores = o.L.zgo_num_threads()
     out = {
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus, "steps": args.steps,
-        "warmup": args.warmup, "ms_per_step": 1000.0 / value, "higher_is_better": True, "scaling": "weak",
-        "vs_baseline": None, "dtype": "u64", "data": "synthetic (seeded random payload bytes)",
+        "warmup": args.warmup, "ms_per_step": 1000.0 * total / args.steps, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "u64", "data": "synthetic (seeded random payload bytes)",
         "config": CONFIG, "impl": "reference",
-        "cpu_baseline": {"value": value, "unit": UNIT, "cores": cores, "kind": "port", "sample": sample},
+        "cpu_baseline": {"value": value, "unit": UNIT, "cores": cores, "kind": "port",
+                         "sample": CPU_SAMPLE + f"; value = ({args.steps} steps / 3) blobs / timed seconds",
+                         "params_build_s": t_params,
+                         "step_s": {"min": min(times), "max": max(times)}},
         "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
     print(json.dumps(out), flush=True)
@@ -742,21 +756,19 @@ def main():
     }
     out.update(extra)
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
-        S = args.cpu_sample or auto_sample()
-        chunks = cpu_sample_chunks(S)
-        Lines = LOG_ROW + 2
-        C = 1 << LOG_COL
-        parts = []
-        for cb in chunks:
-            c, b = divmod(cb, R)
-            for l in range(Lines):
-                parts.append(params.param_line(c, l, first=b * C, count=C))
-        v, cores, detail = cpu_baseline_run(payload.tobytes(), b"".join(parts), chunks)
+        # one full blob (3 coset steps) of the restated CPU path on all host
+        # threads, the same payload: its file root must equal the GPU's
+        o = cpu_oracle()
+        t0 = time.perf_counter()
+        oparams = o.params(LOG_ROW, LOG_COL, PARAM_SEED)
+        t_params = time.perf_counter() - t0
+        v, total, times, root = cpu_blob_steps(o, oparams, payload.tobytes(), 0, 3)
+        gpu_root = pkg.EncoderService(params).process_data(payload.tobytes(), False).storage_root
         out["cpu_baseline"] = {
-            "value": v, "unit": UNIT, "cores": cores, "kind": "port",
-            "sample": f"full RS extension + Merkle of 1 blob, MSM work sampled as {S} of 3072 chunk groups "
-                      f"(12 line-MSMs of 1024 points, this run's params) scaled by 3072/{S}",
-            "detail": detail,
+            "value": v, "unit": UNIT, "cores": o.L.zgo_num_threads(), "kind": "port",
+            "sample": "1 full blob (3 coset steps): " + CPU_SAMPLE,
+            "detail": {"blob_s": total, "coset_step_s": times, "params_build_s": t_params,
+                       "file_root_matches_gpu": root == gpu_root},
         }
     if rank == 0:
         print(json.dumps(out), flush=True)

@@ -6,7 +6,7 @@
  *   - EncoderService::process_data(&[u8], bool)        grpc/src/service.rs:67-105
  *   - EncodedBlob::build / get_row / get_commitment /
  *     get_roots / get_file_root / get_data             crates/encoder/src/encoder/blob.rs:32-62
- *   - RawData::try_from(&[u8]) -> TooLargeBlob         crates/encoder/src/raw_data.rs:76-95
+ *   - RawData::try_from(&[u8]) -> TooLargeBlob         crates/encoder/src/raw_data.rs:55-72
  *   - ZgEncoderParams::from_dir_mont(dir, .., None)    crates/amt/src/blob/encode.rs:114-132
  *   - AMTProofs::gen_amt_proofs (plugin point)         crates/amt/src/prove_params/interfaces.rs:7-15
  * Every entry point below names the reference item it replaces. Plain
@@ -212,10 +212,15 @@ int zg_ctx_msm(zg_ctx* ctx, uint32_t coset, uint32_t line, const void* d_scalars
  * 4 FailedLowDegreeTest), [1..3] the variant's integers (indices and sizes,
  * d of KzgError in [3]). The AMT pairing and MSM checks of all slices are
  * folded into random linear combinations (the reference's DeferredVerifier,
- * crates/amt/src/deferred_verification.rs:67-146) with 128-bit coefficients
- * from `seed` (0: from the OS), and bisected down to single slices when a
- * combination fails, so every code is the one EncodedSlice::verify returns
- * (up to the 2^-128 chance of a false accept). Needs the fixed-base tables.
+ * crates/amt/src/deferred_verification.rs:67-146) with 128-bit coefficients,
+ * and bisected down to single slices when a combination fails, so every code
+ * is the one EncodedSlice::verify returns. With seed == 0 every coefficient
+ * is drawn from the operating system's CSPRNG (getrandom, like the
+ * reference's OsRng draws), and a combination accepts a failing batch with
+ * probability at most 2^-128. A nonzero seed makes the coefficients a
+ * SplitMix64 stream at that seed: reproducible, for tests only, and NOT safe
+ * against slices crafted by anyone who knows the seed. Needs the fixed-base
+ * tables.
  * Returns ZG_OK once every slice has its verdict. */
 #define ZG_V_OK 0
 #define ZG_V_UNMATCHED_AMT_INDEX 1
@@ -262,9 +267,12 @@ int zg_msm_chunks(const void* d_bases, const void* d_scalars, uint32_t lines, ui
  * allocate device memory per call, such as a process that has handed all
  * free HBM to another allocator at start-up, or a loop that must never block
  * on cudaMalloc (which can synchronize the device).
- * The first call on a device looks the array's device address up
- * (cudaGetSymbolAddress) with that device current; make that first call
- * before any stream capture. Every call on a device shares the one array
+ * Every call looks the array's device address up (cudaGetSymbolAddress)
+ * with the call's device current; the first call on a device also loads the
+ * module there, so make that first call before any stream capture. The
+ * array is the module's, so it does not survive cudaDeviceReset; the next
+ * call after a reset finds the reloaded module's array. Every call on a
+ * device shares the one array
  * (it keeps the last call's contents; every element is written before it is
  * read, so nothing needs clearing), so calls that overlap on the GPU, e.g. on
  * two streams at once, race: order them on one stream or with events. */

@@ -427,67 +427,98 @@ void zgo_random_points(uint64_t seed, size_t n, uint8_t* out) {
 }
 
 // ---- CPU baseline ---------------------------------------------------------------
-// Times the restated CPU path on one blob with the MSM work sampled:
-//   t[0] RS extension (RawData -> RawBlob -> 3 cosets, to_coset_blob with
-//        ark-poly style radix-2 transforms) plus Fr -> h256 conversion, full
-//   t[1] keccak Merkle tree, full
-//   t[2] wall time of `S` chunk groups, each the L line-MSMs of one
-//        C-point chunk (the AMT plugin decomposition, prove_gpu.rs:55-87),
-//        run in parallel over all OpenMP threads
-// sample_bases holds, per sampled group, its L lines x C points (mont x||y);
-// sample_chunks[i] = coset * R + chunk.
-int zgo_cpu_baseline(int log_row, int log_col, const uint8_t* data, size_t len, const uint8_t* sample_bases,
-                     const uint32_t* sample_chunks, size_t S, double* t) {
-  Dims d = {log_row, log_col};
-  const size_t N = d.n(), C = d.cols(), R = d.rows();
-  const int L = log_row + 2;
-  double t0 = omp_get_wtime();
-  std::vector<uint8_t> raw;
-  if (!raw_data_from_bytes(d, data, len, &raw)) return -1;
-  std::vector<Fr> blob = raw_blob_from_raw_data(d, raw);
-  std::vector<Fr> points = blob;
-  change_matrix_direction(points, log_col, log_row);
-  std::vector<std::vector<Fr>> cos(COSET_N);
-  for (int c = 0; c < COSET_N; ++c) cos[c] = to_coset_blob(points, c);
-  std::vector<H256> h(COSET_N * N);
-  for (int c = 0; c < COSET_N; ++c) {
-    std::vector<Fr> rm = cos[c];
-    change_matrix_direction(rm, log_row, log_col);
+// The restated CPU path of EncoderService::process_data (grpc/src/service.rs:
+// 69-105) on full blobs, cut into steps of one coset each so that a timing
+// run can stop at any step without extrapolating: three consecutive steps
+// are exactly one blob.
+//   coset 0: RawData::try_from + RawBlob::from (raw_data.rs:55-72,
+//            raw_blob.rs:33-40), change_matrix_direction, then coset 0's
+//            half blob (encode.rs:91-108, 171-183: to_coset_blob, index_reverse,
+//            gen_all_proofs with the prove.rs:58-102 decomposition, every MSM
+//            the ark-style bucket method of zgo_curve.hpp);
+//   coset 1: coset 1's half blob;
+//   coset 2: coset 2's half blob, assert_commitment_consistent, the keccak
+//            Merkle tree (merkle/blob.rs:15-34), the file root and the 3072
+//            ark-serialized slices of the reply (service.rs:85-95).
+struct CpuJob {
+  ParamsHandle* ph = nullptr;
+  std::vector<uint8_t> payload;
+  std::vector<Fr> points;  // column-major blob of the current blob
+  EncodedBlob blob;
+  int next = 0;            // coset of the next step
+  uint8_t file_root[32] = {0};
+  size_t reply_bytes = 0;
+};
+void* zgo_cpu_job_new(void* params, const uint8_t* data, size_t len) {
+  auto* j = new CpuJob();
+  j->ph = static_cast<ParamsHandle*>(params);
+  j->payload.assign(data, data + len);
+  return j;
+}
+void zgo_cpu_job_free(void* job) { delete static_cast<CpuJob*>(job); }
+// Runs the job's next step; returns the coset it covered (0, 1, 2) or -1 when
+// the payload is too large. After a coset-2 step file_root (32 B) and
+// reply_bytes (total serialized slice bytes) describe the finished blob.
+int zgo_cpu_job_step(void* job, uint8_t* file_root, size_t* reply_bytes) {
+  auto* j = static_cast<CpuJob*>(job);
+  const Dims& d = j->ph->d;
+  const int c = j->next;
+  if (c == 0) {
+    std::vector<uint8_t> raw;
+    if (!raw_data_from_bytes(d, j->payload.data(), j->payload.size(), &raw)) return -1;
+    j->points = raw_blob_from_raw_data(d, raw);
+    change_matrix_direction(j->points, d.log_col, d.log_row);
+    j->blob = EncodedBlob();
+    j->blob.dims = d;
+  }
+  j->blob.halves[c] = half_blob_generate(d, to_coset_blob(j->points, c), j->ph->amt[c]);
+  if (c == COSET_N - 1) {
+    for (int k = 1; k < COSET_N; ++k)
+      if (j->blob.halves[k].commitment != j->blob.halves[0].commitment) abort();
+    const size_t n = d.n();
+    std::vector<H256> data(COSET_N * n);
 #pragma omp parallel for schedule(static)
-    for (size_t i = 0; i < N; ++i) h[c * N + i] = scalar_to_h256(rm[i]);
-  }
-  double t1 = omp_get_wtime();
-  Merkle m = merkle_build(d, std::move(h));
-  double t2 = omp_get_wtime();
-  std::vector<std::vector<BigInt>> sc(COSET_N);
-  for (int c = 0; c < COSET_N; ++c) {
-    std::vector<Fr> ri = cos[c];
-    index_reverse(ri);
-    sc[c] = to_bigints(ri.data(), ri.size());
-  }
-  double t3 = omp_get_wtime();
-  std::vector<G1J> out(S * L);
-#pragma omp parallel for schedule(dynamic)
-  for (size_t task = 0; task < S * L; ++task) {
-    size_t gi = task / L, l = task % L;
-    uint32_t cb = sample_chunks[gi];
-    size_t c = cb / R, b = cb % R;
-    std::vector<G1A> bases(C);
-    const uint8_t* src = sample_bases + ((gi * L + l) * C) * 64;
-    for (size_t i = 0; i < C; ++i) {
-      u64 x[4], y[4];
-      memcpy(x, src + 64 * i, 32);
-      memcpy(y, src + 64 * i + 32, 32);
-      bases[i] = {Fq::from_raw_mont(x), Fq::from_raw_mont(y), false};
+    for (size_t i = 0; i < COSET_N * n; ++i) data[i] = scalar_to_h256(j->blob.halves[i / n].blob[i % n]);
+    j->blob.merkle = merkle_build(d, std::move(data));
+    H256 roots[COSET_N] = {j->blob.merkle.tree[0][0], j->blob.merkle.tree[0][1], j->blob.merkle.tree[0][2]};
+    H256 fr = compute_file_root(roots);
+    memcpy(j->file_root, fr.data(), 32);
+    const size_t ns = COSET_N * d.rows();
+    std::vector<size_t> sizes(ns);
+#pragma omp parallel for schedule(dynamic, 16)
+    for (size_t i = 0; i < ns; ++i) {
+      std::vector<uint8_t> v;
+      serialize_slice(encoded_blob_get_row(j->blob, i), v);
+      sizes[i] = v.size();
     }
-    out[task] = msm(bases.data(), sc[c].data() + b * C, C);
+    j->reply_bytes = 0;
+    for (size_t x : sizes) j->reply_bytes += x;
   }
-  double t4 = omp_get_wtime();
-  t[0] = t1 - t0;
-  t[1] = t2 - t1;
-  t[2] = t4 - t3;
-  (void)m;
-  return 0;
+  j->next = (c + 1) % COSET_N;
+  if (file_root) memcpy(file_root, j->file_root, 32);
+  if (reply_bytes) *reply_bytes = j->reply_bytes;
+  return c;
+}
+
+// All slices of an oracle blob back to back (3R x slice size), serialized in
+// parallel: the full-blob comparison of the production tests.
+size_t zgo_blob_all_slices(void* b, uint8_t* out, size_t cap) {
+  auto& blob = static_cast<BlobHandle*>(b)->blob;
+  const size_t ns = COSET_N * blob.dims.rows();
+  std::vector<uint8_t> first;
+  serialize_slice(encoded_blob_get_row(blob, 0), first);
+  const size_t sz = first.size();
+  if (!out) return ns * sz;
+  if (cap < ns * sz) return 0;
+  bool ok = true;
+#pragma omp parallel for schedule(dynamic, 16) reduction(&& : ok)
+  for (size_t i = 0; i < ns; ++i) {
+    std::vector<uint8_t> v;
+    serialize_slice(encoded_blob_get_row(blob, i), v);
+    if (v.size() != sz) { ok = false; continue; }
+    memcpy(out + i * sz, v.data(), sz);
+  }
+  return ok ? ns * sz : 0;
 }
 
 // ---- recovery -----------------------------------------------------------------

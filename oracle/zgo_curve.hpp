@@ -59,7 +59,29 @@ struct Jac {  // (X/Z^2, Y/Z^3); Z == 0 is infinity
     F Z3 = ((Z + o.Z).sqr() - Z1Z1 - Z2Z2) * H;
     return {X3, Y3, Z3};
   }
-  Jac add_affine(const Affine<F>& a) const { return add(from_affine(a)); }
+  // this + affine point (madd-2007-bl: 7M + 4S, the mixed addition ark-ec 0.4
+  // uses for `Projective += &Affine`), with the equal / opposite cases
+  Jac add_affine(const Affine<F>& a) const {
+    if (a.inf) return *this;
+    if (is_inf()) return from_affine(a);
+    F Z1Z1 = Z.sqr();
+    F U2 = a.x * Z1Z1;
+    F S2 = a.y * Z * Z1Z1;
+    if (U2 == X) {
+      if (S2 == Y) return dbl();
+      return inf();
+    }
+    F H = U2 - X;
+    F HH = H.sqr();
+    F I = HH.dbl().dbl();
+    F J = H * I;
+    F r = (S2 - Y).dbl();
+    F V = X * I;
+    F X3 = r.sqr() - J - V.dbl();
+    F Y3 = r * (V - X3) - (Y * J).dbl();
+    F Z3 = (Z + H).sqr() - Z1Z1 - HH;
+    return {X3, Y3, Z3};
+  }
   Jac neg() const { return {X, -Y, Z}; }
   Affine<F> to_affine() const {
     if (is_inf()) return {F::zero(), F::zero(), true};
@@ -144,40 +166,70 @@ static inline bool g2_on_curve(const G2A& p) {
 }
 
 // ---------------------------------------------------------------------------
-// Multi-scalar multiplication (the reference calls ark-ec VariableBaseMSM::msm,
-// crates/amt/src/prove_params/prove.rs:17,31,55,77). Pippenger with unsigned
-// windows; the result is a group element, unique whatever the algorithm.
+// Multi-scalar multiplication: a restatement of the algorithm behind the
+// reference's MSM calls (VariableBaseMSM::msm, crates/amt/src/prove_params/
+// prove.rs:17,31,55,77), ark-ec 0.4.2's signed-digit bucket method for curves
+// with cheap negation (msm_bigint_wnaf; ark-ec is a third-party dependency,
+// Cargo.lock:180, not present here, so this follows its published algorithm):
+//  * window width c = 3 below 32 points, else floor(ceil_log2(n) * 69 / 100) + 2
+//    (ark's ln_without_floats(n) + 2);
+//  * every scalar is cut into ceil(254 / c) signed digits in
+//    [-2^(c-1), 2^(c-1)) read word-wise from its 64-bit limbs, the carry of
+//    the last window folded into the last digit (ark's make_digits);
+//  * per window (in parallel over windows, as ark's `parallel` feature runs
+//    them): 2^c Jacobian buckets, bucket |d| - 1 += +-base with a mixed
+//    addition, then the running-sum reduction from the top bucket down;
+//  * the window sums are folded from the top window with c doublings each.
+// The result is a group element, the same whatever the algorithm.
+static inline int ark_msm_window(size_t n) {
+  if (n < 32) return 3;
+  int l = 0;
+  while ((size_t(1) << l) < n) ++l;
+  return l * 69 / 100 + 2;
+}
+static inline void signed_digits(const BigInt& s, int c, int count, int32_t* out) {
+  const u64 radix = u64(1) << c, mask = radix - 1;
+  u64 carry = 0;
+  for (int i = 0; i < count; ++i) {
+    const int off = i * c, li = off / 64, sh = off % 64;
+    u64 bits = s.v[li] >> sh;
+    if (sh + c > 64 && li + 1 < 4) bits |= s.v[li + 1] << (64 - sh);
+    const u64 coef = carry + (bits & mask);
+    carry = (coef + radix / 2) >> c;
+    out[i] = (int32_t)((int64_t)coef - (int64_t)(carry << c));
+  }
+  out[count - 1] += (int32_t)(carry << c);
+}
 template <class F>
 static Jac<F> msm(const Affine<F>* bases, const BigInt* scalars, size_t n) {
   if (n == 0) return Jac<F>::inf();
-  int c = 1;
-  while ((size_t(1) << (c + 2)) < n && c < 16) ++c;
-  if (n < 8) {
-    Jac<F> acc = Jac<F>::inf();
-    for (size_t i = 0; i < n; ++i) acc = acc.add(Jac<F>::from_affine(bases[i]).mul(scalars[i]));
-    return acc;
-  }
-  int windows = (256 + c - 1) / c;
-  std::vector<Jac<F>> buckets(size_t(1) << c);
-  Jac<F> total = Jac<F>::inf();
-  for (int w = windows - 1; w >= 0; --w) {
-    for (int k = 0; k < c; ++k) total = total.dbl();
-    for (auto& b : buckets) b = Jac<F>::inf();
+  const int c = ark_msm_window(n);
+  const int count = (254 + c - 1) / c;
+  std::vector<int32_t> dig(n * count);
+#pragma omp parallel for schedule(static) if (n >= 4096)
+  for (size_t i = 0; i < n; ++i) signed_digits(scalars[i], c, count, &dig[i * count]);
+  std::vector<Jac<F>> wsum(count);
+#pragma omp parallel for schedule(dynamic, 1) if (n >= 256)
+  for (int w = 0; w < count; ++w) {
+    std::vector<Jac<F>> buckets(size_t(1) << c, Jac<F>::inf());
     for (size_t i = 0; i < n; ++i) {
-      int bit = w * c;
-      u64 d = 0;
-      for (int k = 0; k < c && bit + k < 256; ++k)
-        d |= ((scalars[i].v[(bit + k) / 64] >> ((bit + k) % 64)) & 1) << k;
-      if (d) buckets[d] = buckets[d].add_affine(bases[i]);
+      const int32_t d = dig[i * count + w];
+      if (d > 0) buckets[d - 1] = buckets[d - 1].add_affine(bases[i]);
+      else if (d < 0) buckets[-d - 1] = buckets[-d - 1].add_affine(affine_neg(bases[i]));
     }
-    Jac<F> run = Jac<F>::inf(), sum = Jac<F>::inf();
-    for (size_t b = buckets.size() - 1; b >= 1; --b) {
+    Jac<F> run = Jac<F>::inf(), acc = Jac<F>::inf();
+    for (size_t b = buckets.size(); b-- > 0;) {
       run = run.add(buckets[b]);
-      sum = sum.add(run);
+      acc = acc.add(run);
     }
-    total = total.add(sum);
+    wsum[w] = acc;
   }
-  return total;
+  Jac<F> total = Jac<F>::inf();
+  for (int w = count - 1; w >= 1; --w) {
+    total = total.add(wsum[w]);
+    for (int k = 0; k < c; ++k) total = total.dbl();
+  }
+  return total.add(wsum[0]);
 }
 
 }  // namespace zgo

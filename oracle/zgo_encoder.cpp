@@ -494,7 +494,12 @@ std::vector<BigInt> to_bigints(const Fr* s, size_t n) {
   return out;
 }
 
-// crates/amt/src/prove_params/prove.rs:20-102 (the CPU plugin of AMTProofs)
+// crates/amt/src/prove_params/prove.rs:20-102 (the CPU plugin of AMTProofs).
+// The reference maps over a layer's MSMs one after the other and each MSM
+// runs its windows in parallel (ark-ec's `parallel` feature); so does this
+// restatement, except that MSMs of fewer than 256 points (test shapes only:
+// a layer's MSMs hold at least 1024 points at the production shape) run side
+// by side instead, since their windows are too small to split.
 AllProofs gen_all_proofs(const AMTParams& amt, const std::vector<Fr>& ri, G1J* commitment) {
   size_t len = amt.len();
   size_t batch = len / (size_t(1) << amt.quotients.size());
@@ -507,7 +512,7 @@ AllProofs gen_all_proofs(const AMTParams& amt, const std::vector<Fr>& ri, G1J* c
     size_t items = size_t(1) << depth;
     size_t chunk = len / items;
     std::vector<G1J> q(items);
-#pragma omp parallel for schedule(dynamic)
+#pragma omp parallel for schedule(dynamic) if (chunk < 256)
     for (size_t k = 0; k < items; ++k)
       q[k] = msm(amt.quotients[depth - 1].data() + k * chunk, sc.data() + k * chunk, chunk);
     std::vector<G1A> qa(items);
@@ -517,7 +522,7 @@ AllProofs gen_all_proofs(const AMTParams& amt, const std::vector<Fr>& ri, G1J* c
   // gen_commitment_tree + build_commitment_tree
   size_t nb = len / batch;
   std::vector<G1J> last(nb);
-#pragma omp parallel for schedule(dynamic)
+#pragma omp parallel for schedule(dynamic) if (batch < 256)
   for (size_t k = 0; k < nb; ++k) last[k] = msm(amt.basis.data() + k * batch, sc.data() + k * batch, batch);
   std::vector<G1A> layer(nb);
   normalize_batch(last.data(), layer.data(), nb);

@@ -91,46 +91,93 @@ struct Fp {
   bool operator==(const Fp& o) const { return memcmp(v, o.v, 32) == 0; }
   bool operator!=(const Fp& o) const { return !(*this == o); }
 
+  // add / sub / mul: unrolled four-limb code with u128 carries and a final
+  // conditional subtraction chosen by mask (same values as the textbook
+  // forms; both moduli are below 2^254, so a + b < 2^255 never carries out)
+  static inline void sub_p_if_geq(u64 r[4]) {
+    u128 t = (u128)r[0] - C::P[0];
+    const u64 d0 = (u64)t;
+    t = (u128)r[1] - C::P[1] - (u64)((t >> 64) & 1);
+    const u64 d1 = (u64)t;
+    t = (u128)r[2] - C::P[2] - (u64)((t >> 64) & 1);
+    const u64 d2 = (u64)t;
+    t = (u128)r[3] - C::P[3] - (u64)((t >> 64) & 1);
+    const u64 d3 = (u64)t;
+    const u64 keep = (u64)0 - (u64)((t >> 64) & 1);  // all ones when r < P
+    r[0] = (r[0] & keep) | (d0 & ~keep);
+    r[1] = (r[1] & keep) | (d1 & ~keep);
+    r[2] = (r[2] & keep) | (d2 & ~keep);
+    r[3] = (r[3] & keep) | (d3 & ~keep);
+  }
   Fp operator+(const Fp& o) const {
     Fp r;
-    u64 c = big_add(r.v, v, o.v);
-    if (c || big_geq(r.v, C::P)) big_sub(r.v, r.v, C::P);
+    u128 t = (u128)v[0] + o.v[0];
+    r.v[0] = (u64)t;
+    t = (u128)v[1] + o.v[1] + (u64)(t >> 64);
+    r.v[1] = (u64)t;
+    t = (u128)v[2] + o.v[2] + (u64)(t >> 64);
+    r.v[2] = (u64)t;
+    r.v[3] = v[3] + o.v[3] + (u64)(t >> 64);
+    sub_p_if_geq(r.v);
     return r;
   }
   Fp operator-(const Fp& o) const {
     Fp r;
-    u64 b = big_sub(r.v, v, o.v);
-    if (b) big_add(r.v, r.v, C::P);
+    u128 t = (u128)v[0] - o.v[0];
+    r.v[0] = (u64)t;
+    t = (u128)v[1] - o.v[1] - (u64)((t >> 64) & 1);
+    r.v[1] = (u64)t;
+    t = (u128)v[2] - o.v[2] - (u64)((t >> 64) & 1);
+    r.v[2] = (u64)t;
+    t = (u128)v[3] - o.v[3] - (u64)((t >> 64) & 1);
+    r.v[3] = (u64)t;
+    const u64 m = (u64)0 - (u64)((t >> 64) & 1);  // all ones on borrow: add P back
+    t = (u128)r.v[0] + (C::P[0] & m);
+    r.v[0] = (u64)t;
+    t = (u128)r.v[1] + (C::P[1] & m) + (u64)(t >> 64);
+    r.v[1] = (u64)t;
+    t = (u128)r.v[2] + (C::P[2] & m) + (u64)(t >> 64);
+    r.v[2] = (u64)t;
+    r.v[3] = r.v[3] + (C::P[3] & m) + (u64)(t >> 64);
     return r;
   }
   Fp operator-() const {
     if (is_zero()) return *this;
     Fp r; big_sub(r.v, C::P, v); return r;
   }
-  // CIOS Montgomery multiplication.
+  // CIOS Montgomery multiplication, rows unrolled. The top limb of both
+  // moduli is below 2^62, so the running value never needs a fifth limb
+  // beyond one carry word (the "no-carry" form of CIOS).
   Fp operator*(const Fp& o) const {
-    u64 t[6] = {0, 0, 0, 0, 0, 0};
+    u64 t0 = 0, t1 = 0, t2 = 0, t3 = 0;
     for (int i = 0; i < 4; ++i) {
-      u64 carry = 0;
-      for (int j = 0; j < 4; ++j) {
-        u128 s = (u128)v[j] * o.v[i] + t[j] + carry;
-        t[j] = (u64)s; carry = (u64)(s >> 64);
-      }
-      u128 s = (u128)t[4] + carry;
-      t[4] = (u64)s; t[5] = (u64)(s >> 64);
-      u64 m = t[0] * C::INV;
-      u128 s2 = (u128)m * C::P[0] + t[0];
-      carry = (u64)(s2 >> 64);
-      for (int j = 1; j < 4; ++j) {
-        u128 s3 = (u128)m * C::P[j] + t[j] + carry;
-        t[j - 1] = (u64)s3; carry = (u64)(s3 >> 64);
-      }
-      u128 s4 = (u128)t[4] + carry;
-      t[3] = (u64)s4;
-      t[4] = t[5] + (u64)(s4 >> 64);
+      const u64 bi = o.v[i];
+      u128 x = (u128)v[0] * bi + t0;
+      const u64 a0 = (u64)x;
+      u64 A = (u64)(x >> 64);
+      const u64 m = a0 * C::INV;
+      u128 y = (u128)m * C::P[0] + a0;
+      u64 Cc = (u64)(y >> 64);
+      x = (u128)v[1] * bi + t1 + A;
+      A = (u64)(x >> 64);
+      y = (u128)m * C::P[1] + (u64)x + Cc;
+      Cc = (u64)(y >> 64);
+      t0 = (u64)y;
+      x = (u128)v[2] * bi + t2 + A;
+      A = (u64)(x >> 64);
+      y = (u128)m * C::P[2] + (u64)x + Cc;
+      Cc = (u64)(y >> 64);
+      t1 = (u64)y;
+      x = (u128)v[3] * bi + t3 + A;
+      A = (u64)(x >> 64);
+      y = (u128)m * C::P[3] + (u64)x + Cc;
+      Cc = (u64)(y >> 64);
+      t2 = (u64)y;
+      t3 = Cc + A;
     }
-    Fp r; memcpy(r.v, t, 32);
-    if (t[4] || big_geq(r.v, C::P)) big_sub(r.v, r.v, C::P);
+    Fp r;
+    r.v[0] = t0; r.v[1] = t1; r.v[2] = t2; r.v[3] = t3;
+    sub_p_if_geq(r.v);
     return r;
   }
   Fp& operator+=(const Fp& o) { *this = *this + o; return *this; }

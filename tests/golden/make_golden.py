@@ -1,5 +1,10 @@
-"""Generates tests/golden/encode_3x5.json with an independent pure-Python
-restatement of the encode path at an 8 x 32 blob (LOG_ROW = 3, LOG_COL = 5).
+"""Generates the golden fixtures of tests/golden/ with an independent pure-
+Python restatement of the encode path:
+  encode_3x5.json  an 8 x 32 blob (LOG_ROW = 3, LOG_COL = 5), plus single
+                   known-answer vectors (keccak, G1 multiples, roots);
+  encode_6x5.json  a 64 x 32 blob, the reference's own test setting
+                   (BLOB_ROW_LOG = 6, BLOB_COL_LOG = 5 when TEST_SETTING,
+                   crates/encoder/src/constants.rs:11-15), full payload.
 
 It shares no code with oracle/ or the CUDA library: Python integers for Fr,
 Fq and G1, naive O(n^2) DFTs, a pure-Python Keccak-f[1600], and params from
@@ -14,11 +19,12 @@ import os
 R_MOD = 21888242871839275222246405745257275088548364400416034343698204186575808495617
 Q_MOD = 21888242871839275222246405745257275088696311157297823662689037894645226208583
 G1 = (1, 2)
-LOG_ROW, LOG_COL, COSET_N = 3, 5, 3
-ROWS, COLS = 1 << LOG_ROW, 1 << LOG_COL
-N = ROWS * COLS
-SEED = 42
-PAYLOAD = bytes((i * 7 + 3) % 251 for i in range(200))
+COSET_N = 3
+# the shapes of the fixtures: (file, log_row, log_col, seed, payload)
+FIXTURES = [
+    ("encode_3x5.json", 3, 5, 42, bytes((i * 7 + 3) % 251 for i in range(200))),
+    ("encode_6x5.json", 6, 5, 222, bytes((i * 131 + 17) % 256 for i in range(31 * 2048 - 4))),
+]
 
 
 # ---- Keccak-256 (tiny-keccak Keccak::v256: rate 136, pad 0x01 .. 0x80)
@@ -116,7 +122,10 @@ def root(log_n):
 
 def dft(v, w):
     n = len(v)
-    return [sum(v[j] * pow(w, j * k, R_MOD) for j in range(n)) % R_MOD for k in range(n)]
+    wp = [1] * n  # w^e for e < n (w has order n)
+    for e in range(1, n):
+        wp[e] = wp[e - 1] * w % R_MOD
+    return [sum(v[j] * wp[(j * k) % n] for j in range(n)) % R_MOD for k in range(n)]
 
 
 def idft(v):
@@ -150,7 +159,8 @@ def tau_from_seed(seed):
 
 
 # ---- params in the scalar domain (prove_params/generate.rs:139-263)
-def param_scalars(tau, coset):
+def param_scalars(tau, coset, LOG_ROW, LOG_COL):
+    N = 1 << (LOG_ROW + LOG_COL)
     depth = LOG_ROW + LOG_COL
     w = pow(coset_factor(depth, coset), -1, R_MOD) if coset else 1
     tp = tau * w % R_MOD
@@ -172,7 +182,9 @@ def param_scalars(tau, coset):
 
 
 # ---- encode (crates/amt/src/blob/encode.rs:91-200, encoder/blob.rs:32-72, merkle/blob.rs)
-def encode():
+def encode(LOG_ROW, LOG_COL, SEED, PAYLOAD):
+    ROWS, COLS = 1 << LOG_ROW, 1 << LOG_COL
+    N = ROWS * COLS
     max_blob = 31 * N
     max_raw = max_blob - 4
     raw = bytearray(max_blob)
@@ -190,7 +202,7 @@ def encode():
         g = coset_factor(LOG_ROW + LOG_COL, c) if c else 1
         ev = dft([coeff[m] * pow(g, m, R_MOD) % R_MOD for m in range(N)], root(LOG_ROW + LOG_COL))
         ri = [ev[bitrev(p, LOG_ROW + LOG_COL)] for p in range(N)]
-        basis, quot, high = param_scalars(tau, c)
+        basis, quot, high = param_scalars(tau, c, LOG_ROW, LOG_COL)
         batch = N >> LOG_ROW
         leaves = [sum(ri[k * batch + t] * basis[k * batch + t] for t in range(batch)) % R_MOD
                   for k in range(ROWS)]
@@ -271,7 +283,10 @@ def vectors():
 
 if __name__ == "__main__":
     here = os.path.dirname(os.path.abspath(__file__))
-    out = {"encode": encode(), "vectors": vectors()}
-    with open(os.path.join(here, "encode_3x5.json"), "w") as f:
-        json.dump(out, f, indent=1, sort_keys=True)
-    print("wrote", os.path.join(here, "encode_3x5.json"))
+    for k, (name, lr, lc, seed, payload) in enumerate(FIXTURES):
+        out = {"encode": encode(lr, lc, seed, payload)}
+        if k == 0:
+            out["vectors"] = vectors()
+        with open(os.path.join(here, name), "w") as f:
+            json.dump(out, f, indent=1, sort_keys=True)
+        print("wrote", os.path.join(here, name))

@@ -45,6 +45,16 @@ def empty(n):
     return torch.empty(n, dtype=torch.uint8, device="cuda")
 
 
+def device_view(ptr, n):
+    """A uint8 tensor over n bytes of library-owned device memory."""
+    torch = torch_mod()
+
+    class _Cai:
+        __cuda_array_interface__ = {"shape": (n,), "typestr": "|u1", "data": (ptr, True), "version": 3}
+
+    return torch.as_tensor(_Cai(), device="cuda")
+
+
 def mont_lines(mont: bytes, log_row, log_col):
     """Split a mont params file into its G1 lines (fast_serde_bn254.rs:20-53)."""
     n = 1 << (log_row + log_col)
@@ -408,7 +418,30 @@ def prod(gpu_pkg):
     params.close()
 
 
+@pytest.fixture(scope="module")
+def prod_oracle(prod, oracle):
+    """The oracle's own params of the same seeded tau (built on the CPU) and
+    its full encode of the production payload (the reference CPU
+    decomposition of prove.rs, every MSM ark-ec's signed-digit method)."""
+    _, seed, payload, _ = prod
+    op = oracle.params(10, 10, seed)
+    ob = oracle.encode(op, payload)
+    return op, ob
+
+
+def test_production_params_full(prod, prod_oracle):
+    """Every point of every G1 param line of the three cosets (12 lines of
+    2^20 points each) equals the oracle's, byte for byte."""
+    params = prod[0]
+    op = prod_oracle[0]
+    for c in range(3):
+        for line, exp in enumerate(mont_lines(op.mont(c), 10, 10)):
+            assert params.param_line(c, line) == exp, (c, line)
+
+
 def test_production_params_sample(prod, oracle):
+    """Sampled param points against the scalar-domain oracle (s * G1 of the
+    param scalars of the seeded tau), independent of the oracle's EC builder."""
     params, seed, _, _ = prod
     idx = [0, 1, 2, 777, 65535, 524288, 1048575]
     for c in range(3):
@@ -417,6 +450,23 @@ def test_production_params_sample(prod, oracle):
             exp = oracle.param_points(10, 10, seed, c, line, idx)
             for k, i in enumerate(idx):
                 assert got[64 * i:64 * i + 64] == exp[64 * k:64 * k + 64], (c, line, i)
+
+
+def test_production_full_blob_matches_oracle(prod, prod_oracle):
+    """The whole 1024 x 1024 reply equals the oracle's full encode of the same
+    payload: erasure commitment, storage root, the 96 MiB of encoded data and
+    all 3072 serialized slices (every AMT sibling pair, high commitment, row,
+    Merkle root, path and leaf of every row)."""
+    _, _, _, reply = prod
+    ob = prod_oracle[1]
+    assert reply.erasure_commitment == ob.commitment()
+    assert reply.storage_root == ob.file_root()
+    assert reply.encoded_data == ob.data()
+    exp = ob.all_slices()
+    size = len(exp) // 3072
+    assert len(reply.encoded_slice) == 3072
+    for i, s in enumerate(reply.encoded_slice):
+        assert s == exp[i * size:(i + 1) * size], f"slice {i}"
 
 
 def test_production_encoded_data(prod, oracle):
@@ -455,34 +505,34 @@ def test_production_merkle(prod, oracle):
     assert reply.storage_root == oracle.keccak256(oracle.keccak256(roots[:64]) + roots[64:])
 
 
-def test_production_amt_scalar_domain(prod, oracle):
-    """Every AMT output (commitment tree, proof layers, high commitment) equals
-    (sum_t scalar_t * s_t) * G1 where s_t are the param scalars of the seeded tau."""
-    params, seed, _, reply = prod
+def test_production_amt_scalar_domain(prod, prod_oracle, gpu_pkg, oracle):
+    """Every AMT output of all three cosets -- the commitment tree, the ten
+    proof layers and the high commitment, 3 x (4R - 2) nodes -- equals
+    (sum_t scalar_t * s_t) * G1 with s_t the param scalars of the seeded tau,
+    both as the device wrote them (zg_encode_device) and as the oracle's
+    EC-domain encode computed them, and the commitment is the reply's."""
+    params, seed, payload, reply = prod
     N = params.dims.raw_blob_size
+    R = 1024
     exp = [oracle.amt_scalar_domain(10, 10, seed, c, reply.encoded_data[c * N * 32:(c + 1) * N * 32])
            for c in range(3)]
     assert exp[0][:64] == exp[1][:64] == exp[2][:64]
     com = exp[0][:64]
-    # reply commitment: x || y without flags
     assert reply.erasure_commitment[:63] == com[:63]
     assert reply.erasure_commitment[63] == com[63] & 0x3f
-    R = 1024
+    torch = torch_mod()
+    L = gpu_pkg.lib()
+    tp = dev(payload)
+    db = gpu_pkg._DeviceBlob()
+    assert L.zg_encode_device(params.handle, ctypes.c_void_p(tp.data_ptr()), len(payload), None,
+                              ctypes.byref(db)) == 0, L.zg_last_error()
+    nodes = host(device_view(db.amt_outputs, 3 * (4 * R - 2) * 64))
+    ob = prod_oracle[1]
     for c in range(3):
-        for local in (0, 1, 513, 1023):
-            s = reply.encoded_slice[c * R + local]
-            rev = int(format(local, "010b")[::-1], 2)
-            after = 96 + 32 * 1024
-            for dd in range(10):
-                lv = rev >> (10 - 1 - dd)
-                node = lv ^ 1
-                ci = 1 + (2 << dd) - 2 + node
-                pi = (2 * R - 1) + (2 << dd) - 2 + node
-                pair = s[after + 8 + 128 * dd: after + 8 + 128 * (dd + 1)]
-                assert pair[:64] == exp[c][64 * ci:64 * ci + 64], (c, local, dd)
-                assert pair[64:] == exp[c][64 * pi:64 * pi + 64], (c, local, dd)
-            high = s[after + 8 + 1280: after + 8 + 1280 + 64]
-            assert high == exp[c][64 * (4 * R - 3):64 * (4 * R - 2)]
+        got = nodes[c * (4 * R - 2) * 64:(c + 1) * (4 * R - 2) * 64]
+        for k in range(4 * R - 2):
+            assert got[64 * k:64 * k + 64] == exp[c][64 * k:64 * k + 64], (c, k)
+        assert ob.amt_outputs(c) == exp[c], c
 
 
 def test_production_slices_verify(prod, oracle):
@@ -524,13 +574,15 @@ def test_production_batch_uneven(prod, gpu_pkg):
         assert g == svc.process_data(p, True)
 
 
-def test_encode_matches_golden_fixture(gpu_pkg):
+@pytest.mark.parametrize("fixture", ["encode_3x5.json", "encode_6x5.json"])
+def test_encode_matches_golden_fixture(gpu_pkg, fixture):
     """The CUDA path against the independent pure-Python restatement's bytes
-    (tests/golden/make_golden.py, 8 x 32 blob)."""
+    (tests/golden/make_golden.py): an 8 x 32 blob and the reference's own
+    64 x 32 test setting with a full payload."""
     import hashlib
     import json
     import os
-    g = json.load(open(os.path.join(os.path.dirname(__file__), "golden", "encode_3x5.json")))["encode"]
+    g = json.load(open(os.path.join(os.path.dirname(__file__), "golden", fixture)))["encode"]
     params = gpu_pkg.ZgEncoderParams.from_seed(g["log_row"], g["log_col"], g["seed"])
     reply = gpu_pkg.EncoderService(params).process_data(bytes.fromhex(g["payload_hex"]), True)
     assert reply.erasure_commitment.hex() == g["erasure_commitment"]

@@ -46,9 +46,57 @@ def test_golden_vectors(oracle):
     assert oracle.root_of_unity(28) == int(v["root_of_unity_28"], 16)
 
 
-def test_golden_encode_3x5(oracle):
-    """Byte parity with the pure-Python restatement (tests/golden/make_golden.py)."""
-    e = GOLDEN["encode"]
+# Published constants of the third-party crates the reference computes with,
+# written out as literals: the oracle is pinned to the published values, not
+# to a recomputation of its own.
+# ark-bn254 0.4.0 FrConfig::TWO_ADIC_ROOT_OF_UNITY (TWO_ADICITY = 28)
+ARK_BN254_FR_TWO_ADIC_ROOT = 19103219067921713944291392827692070036145651957329286315305642004821462161904
+# the BN254 generators of ark-bn254 0.4.0 (g1::G1_GENERATOR_X/Y, g2::G2_GENERATOR_X/Y),
+# the EIP-196 / EIP-197 generators: x = c0 + c1 u over Fq2 = Fq[u] / (u^2 + 1)
+G1_GEN = (1, 2)
+G2_GEN_X = (10857046999023057135944570762232829481370756359578518086990519993285655852781,
+            11559732032986387107991004021392285783925812861821192530917403151452391805634)
+G2_GEN_Y = (8495653923123431417604973247489272438418190587263600148770280649306958101930,
+            4082367875863433681332203403145435568316851327593401208105741076214120093531)
+# ark-serialize 0.4 SWFlags in the top bits of the last byte
+SW_FLAG_Y_NEGATIVE, SW_FLAG_INFINITY = 0x80, 0x40
+
+
+def test_published_constants(oracle):
+    assert oracle.root_of_unity(28) == ARK_BN254_FR_TWO_ADIC_ROOT
+    assert pow(ARK_BN254_FR_TWO_ADIC_ROOT, 1 << 28, R_MOD) == 1
+    assert pow(ARK_BN254_FR_TWO_ADIC_ROOT, 1 << 27, R_MOD) == R_MOD - 1
+    # G1 generator and its negation: x || y little-endian, flag bit 7 iff y > -y
+    g = oracle.g1_mul_gen(1)
+    assert g == G1_GEN[0].to_bytes(32, "little") + G1_GEN[1].to_bytes(32, "little")
+    ng = oracle.g1_mul_gen(R_MOD - 1)
+    assert ng[:63] == (G1_GEN[0].to_bytes(32, "little") + (Q_MOD - 2).to_bytes(32, "little"))[:63]
+    assert ng[63] == ((Q_MOD - 2) >> 248) | SW_FLAG_Y_NEGATIVE
+    assert oracle.g1_mul_gen(0) == bytes(63) + bytes([SW_FLAG_INFINITY])
+    # the G2 generator as the mont params file carries it (ark uncompressed:
+    # x.c0, x.c1, y.c0, y.c1 little-endian, flags in the last byte), and it
+    # lies on the twist y^2 = x^3 + 3 / (9 + u)
+    g2 = oracle.params(2, 3, 1).mont(0)[6:6 + 128]
+    coords = [int.from_bytes(g2[32 * i:32 * i + 32], "little") for i in range(4)]
+    coords[3] &= (1 << 254) - 1
+    assert (coords[0], coords[1]) == G2_GEN_X and (coords[2], coords[3]) == G2_GEN_Y
+
+    def f2mul(a, b):
+        return ((a[0] * b[0] - a[1] * b[1]) % Q_MOD, (a[0] * b[1] + a[1] * b[0]) % Q_MOD)
+
+    xi = (9, 1)
+    xi_inv_n = pow(9 * 9 + 1, -1, Q_MOD)
+    b2 = f2mul((3, 0), (9 * xi_inv_n % Q_MOD, (-xi_inv_n) % Q_MOD))
+    x3 = f2mul(f2mul(G2_GEN_X, G2_GEN_X), G2_GEN_X)
+    assert f2mul(G2_GEN_Y, G2_GEN_Y) == ((x3[0] + b2[0]) % Q_MOD, (x3[1] + b2[1]) % Q_MOD)
+    assert f2mul(xi, (9 * xi_inv_n % Q_MOD, (-xi_inv_n) % Q_MOD)) == (1, 0)
+
+
+@pytest.mark.parametrize("fixture", ["encode_3x5.json", "encode_6x5.json"])
+def test_golden_encode(oracle, fixture):
+    """Byte parity with the pure-Python restatement (tests/golden/make_golden.py)
+    at 8 x 32 and at the reference's own 64 x 32 test setting."""
+    e = json.load(open(os.path.join(HERE, "golden", fixture)))["encode"]
     op = oracle.params(e["log_row"], e["log_col"], e["seed"])
     ob = oracle.encode(op, bytes.fromhex(e["payload_hex"]))
     assert hex(oracle.tau(e["seed"])) == e["tau"]

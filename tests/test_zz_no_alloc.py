@@ -54,9 +54,35 @@ def test_noalloc_msm_matches_allocating_entry_point(pkg, oracle):
         assert _host(got) == _host(ref), f"call {call}"
 
 
+def test_noalloc_msm_at_the_scratch_limit(pkg, oracle):
+    """Exactly 1024 chunk MSMs, the size of the static scratch (its last
+    per-MSM result ends at the array's last byte), twice in a row."""
+    import torch
+    if not torch.cuda.is_available():
+        pytest.fail("GPU test run without a CUDA device")
+    L = pkg.lib()
+    lines, log_nchunks, log_chunk = 1, 10, 4         # 1024 chunk MSMs of 16 points
+    n = (1 << log_nchunks) << log_chunk
+    bases = oracle.random_points(4321, lines * n)
+    tb = _dev(bases)
+    for call, seed in enumerate((21, 22)):
+        rng = np.random.default_rng(seed)
+        sc = rng.integers(0, 256, size=(n, 32), dtype=np.uint8)
+        sc[:, 31] = rng.integers(0, 0x30, size=n, dtype=np.uint8)
+        ts = _dev(sc.tobytes())
+        ref = torch.empty((lines << log_nchunks) * 64, dtype=torch.uint8, device="cuda")
+        got = torch.empty_like(ref)
+        assert L.zg_msm_chunks(tb.data_ptr(), ts.data_ptr(), lines, log_nchunks, log_chunk,
+                               ref.data_ptr(), None) == 0, L.zg_last_error()
+        assert L.zg_msm_chunks_noalloc(tb.data_ptr(), ts.data_ptr(), lines, log_nchunks, log_chunk,
+                                       got.data_ptr(), None) == 0, L.zg_last_error()
+        assert _host(got) == _host(ref), f"call {call}"
+
+
 def test_noalloc_msm_rejects_oversized_requests(pkg):
     L = pkg.lib()
     dummy = ctypes.c_void_p(16)
-    rc = L.zg_msm_chunks_noalloc(dummy, dummy, 2, 10, 6, dummy, None)   # 2048 > 1024 MSMs
-    assert rc != 0
-    assert b"static scratch limit" in L.zg_last_error()
+    for lines, log_nchunks in ((2, 10), (1025, 0)):   # 2048 and 1025 > 1024 MSMs
+        rc = L.zg_msm_chunks_noalloc(dummy, dummy, lines, log_nchunks, 6, dummy, None)
+        assert rc != 0
+        assert b"static scratch limit" in L.zg_last_error()

@@ -46,8 +46,10 @@ _SIGS = {
                                         ctypes.POINTER(ctypes.c_int64)]),
     "zgo_merkle_roots": (None, [ctypes.c_int, ctypes.c_int, ctypes.c_char_p, ctypes.c_char_p]),
     "zgo_verify_params_new": (_P, [ctypes.c_int, ctypes.c_int, ctypes.c_uint64, ctypes.c_char_p]),
-    "zgo_cpu_baseline": (ctypes.c_int, [ctypes.c_int, ctypes.c_int, ctypes.c_char_p, _SZ, ctypes.c_char_p,
-                                        ctypes.POINTER(ctypes.c_uint32), _SZ, ctypes.POINTER(ctypes.c_double)]),
+    "zgo_cpu_job_new": (_P, [_P, ctypes.c_char_p, _SZ]),
+    "zgo_cpu_job_free": (None, [_P]),
+    "zgo_cpu_job_step": (ctypes.c_int, [_P, ctypes.c_char_p, ctypes.POINTER(_SZ)]),
+    "zgo_blob_all_slices": (_SZ, [_P, ctypes.c_char_p, _SZ]),
     "zgo_random_points": (None, [ctypes.c_uint64, _SZ, ctypes.c_char_p]),
     "zgo_recover": (ctypes.c_int, [ctypes.c_int, ctypes.c_int, ctypes.POINTER(ctypes.c_uint64),
                                    ctypes.POINTER(ctypes.c_char_p), ctypes.POINTER(_SZ), _SZ,
@@ -144,6 +146,13 @@ class OracleBlob:
         self.L.zgo_blob_slice(self.h, i, b, n)
         return b.raw
 
+    def all_slices(self):
+        """Every serialized slice, back to back, as one bytes object."""
+        n = self.L.zgo_blob_all_slices(self.h, None, 0)
+        b = ctypes.create_string_buffer(n)
+        assert self.L.zgo_blob_all_slices(self.h, b, n) == n
+        return b.raw
+
     def amt_outputs(self, coset):
         n = self.L.zgo_blob_amt_outputs(self.h, coset, None)
         b = ctypes.create_string_buffer(64 * n)
@@ -153,6 +162,25 @@ class OracleBlob:
     def __del__(self):
         try:
             self.L.zgo_blob_free(self.h)
+        except Exception:
+            pass
+
+
+class CpuJob:
+    def __init__(self, L, handle):
+        self.L, self.h = L, handle
+
+    def step(self):
+        """Runs one coset step; returns (coset, file_root or None, reply bytes)."""
+        root = ctypes.create_string_buffer(32)
+        nbytes = ctypes.c_size_t()
+        c = self.L.zgo_cpu_job_step(self.h, root, ctypes.byref(nbytes))
+        assert c >= 0, "payload too large"
+        return c, (root.raw if c == 2 else None), nbytes.value
+
+    def __del__(self):
+        try:
+            self.L.zgo_cpu_job_free(self.h)
         except Exception:
             pass
 
@@ -253,14 +281,10 @@ class Oracle:
         self.L.zgo_random_points(seed, n, out)
         return out.raw
 
-    def cpu_baseline(self, log_row, log_col, data: bytes, sample_bases: bytes, sample_chunks):
-        """(rs_s, merkle_s, msm_sample_s) of the restated CPU path; see oracle/zgo_capi.cpp."""
-        S = len(sample_chunks)
-        arr = (ctypes.c_uint32 * S)(*sample_chunks)
-        t = (ctypes.c_double * 3)()
-        rc = self.L.zgo_cpu_baseline(log_row, log_col, data, len(data), sample_bases, arr, S, t)
-        assert rc == 0
-        return tuple(t)
+    def cpu_job(self, params, data: bytes):
+        """Step-wise full-blob run of the restated CPU encode path (one coset
+        per step, three steps per blob; see oracle/zgo_capi.cpp)."""
+        return CpuJob(self.L, self.L.zgo_cpu_job_new(params.h, data, len(data)))
 
     def recover(self, log_row, log_col, rows: dict):
         ids = sorted(rows)
