@@ -65,24 +65,51 @@ class _DeviceBlob(ctypes.Structure):
     ]
 
 
+# ZG_MSM_PRODUCT_IMAD / _HYBRID / _FP64 / _W28 / _W28_HYBRID
+MSM_PRODUCTS = ("imad", "hybrid", "fp64", "w28", "w28_hybrid")
+MSM_TASK_SIZES = (32, 48, 64, 96)
+MSM_WIDE_MAX = 5
+
+
 class _Tuning(ctypes.Structure):
     """zg_tuning (include/zg_encoder.h)."""
-    _fields_ = [("msm_product", ctypes.c_uint32), ("ntt_cols_per_cta", ctypes.c_uint32),
-                ("ntt_threads", ctypes.c_uint32), ("msm_ms", ctypes.c_float * 3), ("ntt_ms", ctypes.c_float * 9),
-                ("msm_wide_lines", ctypes.c_uint32)]
-
-
-MSM_PRODUCTS = ("imad", "hybrid", "fp64")  # ZG_MSM_PRODUCT_IMAD / _HYBRID / _FP64
+    _fields_ = [("msm_product", ctypes.c_uint32), ("msm_task", ctypes.c_uint32),
+                ("msm_wide_classes", ctypes.c_uint32), ("ntt_cols_per_cta", ctypes.c_uint32),
+                ("ntt_threads", ctypes.c_uint32), ("msm_ms", ctypes.c_float * len(MSM_PRODUCTS)),
+                ("task_ms", ctypes.c_float * len(MSM_TASK_SIZES)), ("wide_ms", ctypes.c_float * (MSM_WIDE_MAX + 1)),
+                ("ntt_ms", ctypes.c_float * 9), ("msm_wide_lines", ctypes.c_uint32),
+                ("msm_wide_avail", ctypes.c_uint32)]
 
 
 def _tuning_dict(t):
-    return {"msm_product": MSM_PRODUCTS[t.msm_product], "ntt_cols_per_cta": t.ntt_cols_per_cta,
+    return {"msm_product": MSM_PRODUCTS[t.msm_product], "msm_task": t.msm_task,
+            "msm_wide_classes": t.msm_wide_classes, "ntt_cols_per_cta": t.ntt_cols_per_cta,
             "ntt_threads": t.ntt_threads, "msm_ms": [round(x, 4) for x in t.msm_ms],
-            "ntt_ms": [round(x, 4) for x in t.ntt_ms], "msm_wide_lines": t.msm_wide_lines}
+            "task_ms": [round(x, 4) for x in t.task_ms], "wide_ms": [round(x, 4) for x in t.wide_ms],
+            "ntt_ms": [round(x, 4) for x in t.ntt_ms], "msm_wide_lines": t.msm_wide_lines,
+            "msm_wide_avail": t.msm_wide_avail}
+
+
+MAX_FUSED_BLOBS = 2  # ZG_MAX_FUSED_BLOBS
+
+
+class _PipelineConfig(ctypes.Structure):
+    """zg_pipeline_config (include/zg_encoder.h)."""
+    _fields_ = [("max_units", ctypes.c_uint32), ("blobs_per_launch", ctypes.c_uint32),
+                ("reserve_mib", ctypes.c_uint32)]
+
+
+class _PipelineStats(ctypes.Structure):
+    """zg_pipeline_stats (include/zg_encoder.h)."""
+    _fields_ = [("units", ctypes.c_uint64), ("launches", ctypes.c_uint64 * MAX_FUSED_BLOBS),
+                ("max_in_flight", ctypes.c_uint64), ("recoveries", ctypes.c_uint64),
+                ("unit_bytes", ctypes.c_uint64)]
 
 
 _P = ctypes.c_void_p
 _SZ = ctypes.c_size_t
+
+
 class _Request(ctypes.Structure):
     """zg_request (include/zg_encoder.h)."""
     _fields_ = [("kind", ctypes.c_int), ("data", ctypes.c_void_p), ("len", ctypes.c_size_t),
@@ -106,6 +133,8 @@ _SIGS = {
     "zg_verify_slices": (ctypes.c_int, [_P, ctypes.POINTER(ctypes.c_char_p), ctypes.POINTER(_SZ), _SZ,
                                         ctypes.c_char_p, ctypes.c_char_p, ctypes.c_uint64,
                                         ctypes.POINTER(ctypes.c_int32), ctypes.POINTER(ctypes.c_int64)]),
+    "zg_ctx_set_pipeline": (ctypes.c_int, [_P, ctypes.POINTER(_PipelineConfig)]),
+    "zg_ctx_pipeline_stats": (ctypes.c_int, [_P, ctypes.POINTER(_PipelineStats)]),
     "zg_ctx_autotune": (ctypes.c_int, [_P, ctypes.POINTER(_Tuning)]),
     "zg_ctx_get_tuning": (ctypes.c_int, [_P, ctypes.POINTER(_Tuning)]),
     "zg_ctx_set_tuning": (ctypes.c_int, [_P, ctypes.POINTER(_Tuning)]),
@@ -217,9 +246,9 @@ def probe_imad(device=0):
 
 def selftest():
     """Mismatch counts of the device arithmetic against its host build."""
-    fails = (ctypes.c_int * 7)()
-    _check(lib().zg_selftest(fails, 7))
-    return dict(zip(["fq_mul", "fq_mul_f64", "fq_add", "fq_sub", "fr_mul", "fr_roundtrip", "xyzz_dbl"],
+    fails = (ctypes.c_int * 8)()
+    _check(lib().zg_selftest(fails, 8))
+    return dict(zip(["fq_mul", "fq_mul_f64", "fq_add", "fq_sub", "fr_mul", "fr_roundtrip", "xyzz_dbl", "fq_mul_w28"],
                     list(fails)))
 
 
@@ -320,11 +349,31 @@ class ZgEncoderParams:
         _check(lib().zg_ctx_get_tuning(self.handle, ctypes.byref(t)))
         return _tuning_dict(t)
 
-    def set_tuning(self, msm_product="hybrid", ntt_cols_per_cta=2, ntt_threads=256):
+    def set_tuning(self, msm_product="hybrid", ntt_cols_per_cta=2, ntt_threads=256, msm_task=64,
+                   msm_wide_classes=None):
+        """Fix the kernels' free choices (zg_ctx_set_tuning); msm_wide_classes
+        None keeps every wide-window class the context holds."""
+        cur = self.tuning()
         t = _Tuning()
         t.msm_product = MSM_PRODUCTS.index(msm_product)
+        t.msm_task = msm_task
+        t.msm_wide_classes = cur["msm_wide_avail"] if msm_wide_classes is None else msm_wide_classes
         t.ntt_cols_per_cta, t.ntt_threads = ntt_cols_per_cta, ntt_threads
         _check(lib().zg_ctx_set_tuning(self.handle, ctypes.byref(t)))
+
+    def set_pipeline(self, max_units=0, blobs_per_launch=0, reserve_mib=0):
+        """Settings of the request pipeline (zg_ctx_set_pipeline): at most
+        max_units units (0 = as free HBM allows), blobs_per_launch blobs fused
+        per unit launch (0 = MAX_FUSED_BLOBS, 1 = none), reserve_mib of device
+        memory kept free by admission (0 = 4096)."""
+        cfg = _PipelineConfig(max_units, blobs_per_launch, reserve_mib)
+        _check(lib().zg_ctx_set_pipeline(self._h, ctypes.byref(cfg)))
+
+    def pipeline_stats(self):
+        st = _PipelineStats()
+        _check(lib().zg_ctx_pipeline_stats(self._h, ctypes.byref(st)))
+        return {"units": st.units, "launches_by_blobs": {k + 1: st.launches[k] for k in range(MAX_FUSED_BLOBS)},
+                "max_in_flight": st.max_in_flight, "recoveries": st.recoveries, "unit_bytes": st.unit_bytes}
 
     def set_profiling(self, enable=True):
         _check(lib().zg_ctx_set_profiling(self._h, 1 if enable else 0))

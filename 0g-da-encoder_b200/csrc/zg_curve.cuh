@@ -7,6 +7,7 @@
 #pragma once
 #include "zg_field.cuh"
 #include "zg_field_f64.cuh"
+#include "zg_field_w28.cuh"
 
 namespace zg {
 
@@ -14,13 +15,18 @@ namespace zg {
 // functions: the formulas then compile to a few hundred instructions that stay
 // in the instruction cache, instead of ten inlined ~300-instruction products
 // per point addition (host builds inline them). Independent products are
-// issued in pairs. Three interchangeable product kinds (same values):
+// issued in pairs. Five interchangeable product kinds (same values):
 //   MulImad   both products of a pair on the integer multiply-add pipe
 //             (Fq::mul2, the two CIOS carry chains interleaved);
 //   MulHybrid the first on the integer pipe (Fq::mul), the second on the FP64
 //             pipe (f52::mont_mul): the MSM bucket loop saturates the integer
 //             pipe with carry-chain IMADs, so this pair keeps both pipes busy;
-//   MulF64    both on the FP64 pipe.
+//   MulF64    both on the FP64 pipe;
+//   MulW28    both as 28-bit-limb products with 64-bit column sums
+//             (w28::mont_mul: wide multiply-adds without carry flags, the
+//             columns independent chains);
+//   MulW28Hybrid the first as a 28-bit-limb product, the second on the FP64
+//             pipe.
 // The curve formulas are templates over the kind; one kernel uses one kind
 // only (two product functions in one hot loop overflow the instruction
 // cache). MulHybrid is the default; the MSM kernel comes in all three and the
@@ -42,6 +48,19 @@ static __device__ __noinline__ FqPair fq_mul2_hybrid_ool(const Fq a, const Fq b,
   return r;
 }
 static __device__ __noinline__ Fq fq_mul_f64_ool(const Fq a, const Fq b) { return f52::mont_mul(a, b); }
+static __device__ __noinline__ Fq fq_mul_w28_ool(const Fq a, const Fq b) { return w28::mont_mul(a, b); }
+static __device__ __noinline__ FqPair fq_mul2_w28_ool(const Fq a, const Fq b, const Fq c, const Fq d) {
+  FqPair r;
+  r.a = w28::mont_mul(a, b);
+  r.b = w28::mont_mul(c, d);
+  return r;
+}
+static __device__ __noinline__ FqPair fq_mul2_w28f64_ool(const Fq a, const Fq b, const Fq c, const Fq d) {
+  FqPair r;
+  r.a = w28::mont_mul(a, b);
+  r.b = f52::mont_mul(c, d);
+  return r;
+}
 static __device__ __noinline__ FqPair fq_mul2_f64_ool(const Fq a, const Fq b, const Fq c, const Fq d) {
   FqPair r;
   r.a = f52::mont_mul(a, b);
@@ -66,6 +85,18 @@ struct MulF64 {
     return fq_mul2_f64_ool(a, b, c, d);
   }
 };
+struct MulW28 {
+  static __device__ __forceinline__ Fq mul(const Fq& a, const Fq& b) { return fq_mul_w28_ool(a, b); }
+  static __device__ __forceinline__ FqPair mul2(const Fq& a, const Fq& b, const Fq& c, const Fq& d) {
+    return fq_mul2_w28_ool(a, b, c, d);
+  }
+};
+struct MulW28Hybrid {
+  static __device__ __forceinline__ Fq mul(const Fq& a, const Fq& b) { return fq_mul_w28_ool(a, b); }
+  static __device__ __forceinline__ FqPair mul2(const Fq& a, const Fq& b, const Fq& c, const Fq& d) {
+    return fq_mul2_w28f64_ool(a, b, c, d);
+  }
+};
 #else
 // host builds: the same values through Fq::mul; three distinct types so that
 // kernel templates keep one instance per kind in both compilation passes
@@ -80,6 +111,8 @@ struct MulHost {
 struct MulImad : MulHost {};
 struct MulHybrid : MulHost {};
 struct MulF64 : MulHost {};
+struct MulW28 : MulHost {};
+struct MulW28Hybrid : MulHost {};
 #endif
 
 struct G1Aff {

@@ -649,8 +649,8 @@ struct FbAccArgs {
 // Persistent CTAs over the (chunk, line) work items. Per item:
 //  1. every bucket is cut into tasks of at most tsz entries (the top
 //     window's digits are tiny, so buckets 1 and 2 hold ~10x the average);
-//     tsz = FB_TASK unless the item holds more than (FB_MAX_TASKS -
-//     FB_BUCKETS) * FB_TASK entries (wide items of skewed scalars), so an
+//     tsz = task unless the item holds more than (FB_MAX_TASKS -
+//     FB_BUCKETS) * task entries (wide items of skewed scalars), so an
 //     item never has more than FB_MAX_TASKS tasks;
 //  2. tasks are counting-sorted by size and round r gives thread i the task at
 //     sorted position 128 r + i: the 32 lanes of a warp run tasks of nearly
@@ -663,31 +663,37 @@ struct FbAccArgs {
 // 1) of unit g >> (ulog - 10); its buckets' entries index the unit's points
 // and the W windows of the wide table.
 // One launch covers up to FB_MAX_SETS item sets (a blob's chunk items and its
-// wide classes): set k holds items start[k] .. start[k + 1] - 1, described by
-// a[k] with local item index u - start[k]. One launch keeps the persistent
-// CTAs busy to the end of the whole MSM instead of leaving a partial last
-// round per set. A CTA takes its next item from the counter *next (zero at
+// wide classes, for up to FB_MAX_BLOBS blobs whose MSMs share the launch):
+// set k holds items start[k] .. start[k + 1] - 1, described by a[k] with
+// local item index u - start[k]. One launch keeps the persistent CTAs busy to
+// the end of the whole MSM instead of leaving a partial last round per set. A CTA takes its next item from the counter *next (zero at
 // launch): items differ in size (a wide unit's block 0 holds the top
 // window's digits), and a fixed item-to-CTA map would give some CTAs every
 // heavy item.
-constexpr int FB_MAX_SETS = 8;
+constexpr int FB_MAX_BLOBS = 2;  // blobs per fused MSM launch
+constexpr int FB_MAX_SETS = 8 * FB_MAX_BLOBS;
 struct FbAccPlan {
   int n = 0;
   uint32_t start[FB_MAX_SETS + 1] = {};
   FbAccArgs a[FB_MAX_SETS];
 };
-constexpr int FB_TASK = 64;
-constexpr int FB_MAX_TASKS = FB_BUCKETS + FB_WINDOWS * 1024 / FB_TASK;  // chunk <= 1024 points
+// Bucket task size (entries per task, a tuning choice within [FB_TASK_MIN,
+// FB_TASK_MAX]); the task arrays are sized for the smallest.
+constexpr int FB_TASK_MIN = 32;
+constexpr int FB_TASK_MAX = 96;
+constexpr int FB_TASK_DEFAULT = 64;
+constexpr int FB_MAX_TASKS = FB_BUCKETS + FB_WINDOWS * 1024 / FB_TASK_MIN;  // chunk <= 1024 points
 // M is the product kind of the point additions (MulImad / MulHybrid / MulF64,
 // chosen by the context's tuning; identical results).
 template <class M>
 __global__ void __launch_bounds__(FB_ACC_THREADS, FB_ACC_MIN_CTAS) k_fb_accum(const FbAccPlan plan, XYZZ* __restrict__ gpart_all,
-                                                                uint32_t* __restrict__ next) {
+                                                                uint32_t* __restrict__ next, uint32_t task) {
   __shared__ uint32_t soffs[FB_BUCKETS + 1];
   __shared__ uint16_t tstart[FB_BUCKETS + 1];
   __shared__ uint16_t order[FB_MAX_TASKS];
   __shared__ uint16_t tbucket[FB_MAX_TASKS];
-  __shared__ uint32_t bins[FB_TASK + 1];
+  __shared__ uint32_t bins[FB_TASK_MAX + 1];
+  task = min(max(task, (uint32_t)FB_TASK_MIN), (uint32_t)FB_TASK_MAX);
   __shared__ uint32_t item;
   XYZZ* gpart = gpart_all + (size_t)blockIdx.x * FB_MAX_TASKS;
   const uint32_t units = plan.start[plan.n];
@@ -725,11 +731,11 @@ __global__ void __launch_bounds__(FB_ACC_THREADS, FB_ACC_MIN_CTAS) k_fb_accum(co
     }
     __syncthreads();  // the previous item is finished with the shared arrays and gpart
     for (int k = threadIdx.x; k <= FB_BUCKETS; k += blockDim.x) soffs[k] = offs[k];
-    for (int k = threadIdx.x; k <= FB_TASK; k += blockDim.x) bins[k] = 0;
+    for (int k = threadIdx.x; k <= FB_TASK_MAX; k += blockDim.x) bins[k] = 0;
     __syncthreads();
     const uint32_t nent = soffs[FB_BUCKETS] - soffs[0];
     const uint32_t cap = (uint32_t)(FB_MAX_TASKS - FB_BUCKETS);
-    const uint32_t tsz = max((uint32_t)FB_TASK, (nent + cap - 1) / cap);
+    const uint32_t tsz = max(task, (nent + cap - 1) / cap);
     // tasks per bucket, exclusive scan -> tstart (bucket k = 0-based index)
     if (threadIdx.x < 32) {
       // warp-level scan over 1024 buckets, 32 per lane
@@ -757,20 +763,21 @@ __global__ void __launch_bounds__(FB_ACC_THREADS, FB_ACC_MIN_CTAS) k_fb_accum(co
     __syncthreads();
     const uint32_t ntasks = tstart[FB_BUCKETS];
     // size of task j of bucket k: tsz except the bucket's last task; bin
-    // FB_TASK - size * FB_TASK / tsz (the size itself when tsz = FB_TASK)
+    // task - size * task / tsz (task - size when tsz = task): larger tasks
+    // first
     for (int k = threadIdx.x; k < FB_BUCKETS; k += blockDim.x) {
       const uint32_t c = soffs[k + 1] - soffs[k];
       for (uint32_t t = tstart[k]; t < tstart[k + 1]; ++t) {
         tbucket[t] = (uint16_t)k;
         const uint32_t j = t - tstart[k];
         const uint32_t sz = min(tsz, c - j * tsz);
-        atomicAdd(&bins[FB_TASK - sz * FB_TASK / tsz], 1u);
+        atomicAdd(&bins[task - sz * task / tsz], 1u);
       }
     }
     __syncthreads();
     if (threadIdx.x == 0) {
       uint32_t acc = 0;
-      for (int i = 0; i <= FB_TASK; ++i) { uint32_t v = bins[i]; bins[i] = acc; acc += v; }
+      for (uint32_t i = 0; i <= task; ++i) { uint32_t v = bins[i]; bins[i] = acc; acc += v; }
     }
     __syncthreads();
     for (uint32_t t = threadIdx.x; t < ntasks; t += blockDim.x) {
@@ -778,7 +785,7 @@ __global__ void __launch_bounds__(FB_ACC_THREADS, FB_ACC_MIN_CTAS) k_fb_accum(co
       const uint32_t c = soffs[k + 1] - soffs[k];
       const uint32_t j = t - tstart[k];
       const uint32_t sz = min(tsz, c - j * tsz);
-      order[atomicAdd(&bins[FB_TASK - sz * FB_TASK / tsz], 1u)] = (uint16_t)t;
+      order[atomicAdd(&bins[task - sz * task / tsz], 1u)] = (uint16_t)t;
     }
     __syncthreads();
     for (uint32_t r = threadIdx.x; r < ntasks; r += blockDim.x) {
@@ -826,9 +833,10 @@ __global__ void __launch_bounds__(FB_ACC_THREADS, FB_ACC_MIN_CTAS) k_fb_accum(co
 // 2^lr + b], line = L - 1 for the set's last line when hi_last, else l0 + l.
 // Wide items (block blk = b & (2^bpu_log - 1) of a unit) add 1024 blk *
 // sum_k B_k: their buckets hold digits 1024 blk + k + 1 (bpu_log = 0 for
-// chunk items).
+// chunk items). part_off places a fused launch's blob in its own part block.
 struct FbCombineMap {
   int lr, lines, l0, L, hi_last, bpu_log;
+  uint64_t part_off;
 };
 struct FbCombinePlan {
   int n = 0;
@@ -892,7 +900,7 @@ __global__ void __launch_bounds__(64) k_fb_combine(const XYZZ* __restrict__ T, c
     run.add(load_xyzz(s));  // sum of all the item's buckets
     tot.add(fb_block_term(run, blk));
   }
-  store_xyzz(part + fb_part_index(m, v), tot);
+  store_xyzz(part + m.part_off + fb_part_index(m, v), tot);
 }
 
 __device__ __forceinline__ XYZZ shfl_xor_xyzz(const XYZZ& p, int m) {
@@ -954,7 +962,7 @@ __global__ void __launch_bounds__(128) k_fb_combine_warp(const XYZZ* __restrict_
     tl.add(a);
     const uint32_t blk = fb_item_block(m, v);
     if (blk) tl.add(fb_block_term(U, blk));  // U at lane 0 = sum of all the item's buckets
-    store_xyzz(part + fb_part_index(m, v), tl);
+    store_xyzz(part + m.part_off + fb_part_index(m, v), tl);
   }
 }
 

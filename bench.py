@@ -123,10 +123,10 @@ def parse():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--batch-blobs", type=int, default=8, help="blobs in the batched-uneven sample")
-    ap.add_argument("--serve-rate", default="2,8",
+    ap.add_argument("--batch-blobs", type=int, default=32, help="blobs in the batched-uneven sample")
+    ap.add_argument("--serve-rate", default="3,6,9",
                     help="Poisson arrival rates of the serving sample (1/s, comma-separated sweep)")
-    ap.add_argument("--serve-requests", type=int, default=16, help="requests per serving sample (0 = skip)")
+    ap.add_argument("--serve-requests", type=int, default=128, help="requests per serving sample (0 = skip)")
     ap.add_argument("--no-serve-plain", action="store_true",
                     help="skip serving the same arrivals through the blocking per-blob path")
     ap.add_argument("--verify-sample", type=int, default=4,
@@ -136,7 +136,8 @@ def parse():
                          "points (uniform and blob-like scalars), NTTs (1024 x 2^10, 64 x 2^14, 1 x 2^20; "
                          "forward, inverse, coset), Keccak Merkle over 3072 x 1024 x 32 B")
     ap.add_argument("--tuning", default="",
-                    help="PRODUCT,COLS,THREADS (e.g. hybrid,1,256): use these kernel choices instead of autotuning "
+                    help="PRODUCT,COLS,THREADS[,TASK[,WIDE_CLASSES]] (e.g. hybrid,1,256,64,5): use these kernel "
+                         "choices instead of autotuning "
                          "(profiling runs, where the autotuner's own timings would be distorted)")
     ap.add_argument("--msm-window-bits", type=int, default=0,
                     help="0 = the context's choice (11-bit fixed-base tables when they fit), 8 = 8-bit windows "
@@ -566,8 +567,9 @@ def main():
     # the kernels' free choices (MSM product kind, RS tile shape), timed on a
     # synthetic blob before any measurement
     if args.tuning:
-        prod_kind, cols, threads = args.tuning.split(",")
-        params.set_tuning(prod_kind, int(cols), int(threads))
+        f = args.tuning.split(",")
+        params.set_tuning(f[0], int(f[1]), int(f[2]), msm_task=int(f[3]) if len(f) > 3 else 64,
+                          msm_wide_classes=int(f[4]) if len(f) > 4 else None)
         tuning = dict(params.tuning(), source="--tuning")
     else:
         tuning = params.autotune()
@@ -659,17 +661,54 @@ def main():
     barrier()
     e2e_plain = job_value(world, args.steps, plain_s)
 
-    # batched uneven payloads and a serving sample (single-GPU runs)
+    # batched uneven payloads (one zg_encode_batch call of all the blobs) and
+    # a serving sample (single-GPU runs)
     extra = {}
     if world == 1 and args.batch_blobs > 0:
         sizes = np.random.default_rng(4).integers(64 << 10, PAYLOAD + 1, args.batch_blobs)
+        n = len(sizes)
+        ptrs = (ctypes.c_void_p * n)(*([h_ptr] * n))
+        lens = (ctypes.c_size_t * n)(*[int(x) for x in sizes])
+        outs = (ctypes.c_void_p * n)()
+
+        def batch_call():
+            rc = L.zg_encode_batch(params.handle, n, ptrs, lens, 1, outs)
+            assert rc == 0, L.zg_last_error()
+            for i in range(n):
+                L.zg_reply_free(outs[i])
+
+        modes = {}
+        for name, fuse in (("fused_pairs", 2), ("one_blob_per_launch", 1)):
+            params.set_pipeline(blobs_per_launch=fuse)
+            batch_call()  # units and their graphs come up
+            st0 = params.pipeline_stats()
+            torch.cuda.synchronize()
+            t0 = time.perf_counter()
+            batch_call()
+            bt = time.perf_counter() - t0
+            st1 = params.pipeline_stats()
+            modes[name] = {"value": n / bt, "seconds": bt, "units": st1["units"],
+                           "launches_by_blobs": {k: st1["launches_by_blobs"][k] - st0["launches_by_blobs"][k]
+                                                 for k in st1["launches_by_blobs"]},
+                           "max_in_flight": st1["max_in_flight"]}
+        params.set_pipeline()
         t0 = time.perf_counter()
-        pipeline(sizes)
-        bt = time.perf_counter() - t0
+        for x in sizes:
+            r = ctypes.c_void_p()
+            rc = L.zg_encode(params.handle, ctypes.cast(ctypes.c_void_p(h_ptr), ctypes.c_char_p), int(x), 1,
+                             ctypes.byref(r))
+            assert rc == 0, L.zg_last_error()
+            L.zg_reply_free(r)
+        plain_bt = time.perf_counter() - t0
         extra["batched_uneven"] = {
-            "blobs": int(args.batch_blobs), "value": args.batch_blobs / bt, "unit": UNIT,
+            "blobs": n, "value": modes["fused_pairs"]["value"], "unit": UNIT,
             "payload_mean_bytes": float(sizes.mean()),
-            "path": "pipeline (zg_submit / zg_wait; per-slot CUDA graphs), pinned host payloads, full replies",
+            "path": "zg_encode_batch: pipeline units of 2 blob slots, each pair fused into one launch sequence "
+                    "(one bucket accumulation over both blobs' MSMs) from a captured CUDA graph; pinned host "
+                    "payloads, full replies",
+            "modes": modes,
+            "plain_value": n / plain_bt, "plain_path": "blocking zg_encode per blob",
+            "fused_over_plain": modes["fused_pairs"]["value"] / (n / plain_bt),
         }
     if world == 1 and args.serve_requests > 0:
         rows_reply = pkg.EncoderService(params).process_data(payload.tobytes(), True)
@@ -678,8 +717,13 @@ def main():
         full = payload.tobytes()
         extra["serving"] = []
         for rate in [float(x) for x in str(args.serve_rate).split(",") if x]:
-            extra["serving"].append(serving_run(pkg, params, pipe, h_ptr, full, recs, rate,
-                                                args.serve_requests, 5))
+            st0 = params.pipeline_stats()
+            row = serving_run(pkg, params, pipe, h_ptr, full, recs, rate, args.serve_requests, 5)
+            st1 = params.pipeline_stats()
+            row["pipeline"] = {"units": st1["units"], "max_in_flight": st1["max_in_flight"],
+                               "launches_by_blobs": {k: st1["launches_by_blobs"][k] - st0["launches_by_blobs"][k]
+                                                     for k in st1["launches_by_blobs"]}}
+            extra["serving"].append(row)
             if not args.no_serve_plain:
                 extra["serving"].append(serving_run(pkg, params, pipe, h_ptr, full, recs, rate,
                                                     args.serve_requests, 5, plain=True))

@@ -101,31 +101,57 @@ int zg_ctx_param_points(zg_ctx* ctx, int coset, int line, size_t first, size_t c
 
 /* Tuning of the kernels' free choices (no reference counterpart: the
  * reference's GPU plugin fixes its window width and launch shapes inside
- * ag-cuda-ec, prove_gpu.rs:77). Every choice gives identical results.
+ * ag-cuda-ec, prove_gpu.rs:16-17,77). Every choice gives identical results.
  *   msm_product      field products of the MSM point additions:
  *                    ZG_MSM_PRODUCT_IMAD both products of each independent pair
- *                    on the integer multiply-add pipe, ZG_MSM_PRODUCT_HYBRID one
- *                    there and one on the FP64 pipe (default), ZG_MSM_PRODUCT_FP64
- *                    both on the FP64 pipe;
+ *                    as 32-bit carry-chain CIOS on the integer multiply-add
+ *                    pipe, ZG_MSM_PRODUCT_HYBRID one there and one on the FP64
+ *                    pipe, ZG_MSM_PRODUCT_FP64 both on the FP64 pipe,
+ *                    ZG_MSM_PRODUCT_W28 both as 28-bit-limb products with 64-bit
+ *                    column sums (wide multiply-adds, no carry flags),
+ *                    ZG_MSM_PRODUCT_W28_HYBRID one of those and one on the FP64
+ *                    pipe;
+ *   msm_task         bucket layout: entries per bucket-accumulation task, 32,
+ *                    48, 64 (default) or 96 (buckets are cut into tasks of at
+ *                    most this many points, scheduled by size);
+ *   msm_wide_classes MSM window width per AMT line: how many of the context's
+ *                    wide-window classes are in use, largest unit first (class
+ *                    u gives the lines whose nodes hold >= 2^u points units of
+ *                    2^u points and (u + 1)-bit windows; the lines of the
+ *                    classes not in use run 11-bit windows per 1024-point
+ *                    chunk); at most msm_wide_avail;
  *   ntt_cols_per_cta columns per CTA of the RS column pass: 1, 2 (default), 4;
  *   ntt_threads      threads per CTA of the three RS passes: 128, 256 (default), 512.
  * zg_ctx_autotune encodes a synthetic full-size blob on the context, times
- * each MSM product kind on a sample of the blob's chunk MSMs and each NTT
- * shape on the full RS extension, keeps the fastest and returns the choice
- * with the times (ms; msm_ms[kind], ntt_ms[3 * i + j] for cols_per_cta
- * {1, 2, 4}[i] and threads {128, 256, 512}[j]). It runs after the context's
- * queued work and takes well under a second at production size; the request
- * pipeline re-captures its CUDA graphs for the new choice. */
+ * each MSM product kind on a sample of the blob's MSM items (msm_ms), each
+ * task size with the fastest kind (task_ms, sizes {32, 48, 64, 96}), the
+ * whole blob MSM with 0 .. msm_wide_avail wide classes (wide_ms; -1 where
+ * the context has no such class) and each NTT shape on the full RS
+ * extension (ntt_ms[3 * i + j] for cols_per_cta {1, 2, 4}[i] and threads
+ * {128, 256, 512}[j]), keeps the fastest of each and returns the choice with
+ * the times (ms). It runs after the context's queued work and takes a few
+ * seconds at production size; the request pipeline re-captures its CUDA
+ * graphs for the new choice. */
 #define ZG_MSM_PRODUCT_IMAD 0
 #define ZG_MSM_PRODUCT_HYBRID 1
 #define ZG_MSM_PRODUCT_FP64 2
+#define ZG_MSM_PRODUCT_W28 3
+#define ZG_MSM_PRODUCT_W28_HYBRID 4
+#define ZG_MSM_PRODUCTS 5
+#define ZG_MSM_TASK_SIZES 4
+#define ZG_MSM_WIDE_MAX 5
 typedef struct zg_tuning {
   uint32_t msm_product;
+  uint32_t msm_task;
+  uint32_t msm_wide_classes;
   uint32_t ntt_cols_per_cta;
   uint32_t ntt_threads;
-  float msm_ms[3];
+  float msm_ms[ZG_MSM_PRODUCTS];
+  float task_ms[ZG_MSM_TASK_SIZES];
+  float wide_ms[ZG_MSM_WIDE_MAX + 1];
   float ntt_ms[9];
-  uint32_t msm_wide_lines; /* read-only: AMT lines on wide windows (0 = none) */
+  uint32_t msm_wide_lines; /* read-only: AMT lines on wide windows with the chosen classes */
+  uint32_t msm_wide_avail; /* read-only: wide-window classes whose tables the context holds */
 } zg_tuning;
 int zg_ctx_autotune(zg_ctx* ctx, zg_tuning* out);
 int zg_ctx_get_tuning(zg_ctx* ctx, zg_tuning* out);
@@ -160,10 +186,18 @@ int zg_recover(zg_ctx* ctx, const uint64_t* row_ids, const uint8_t* const* rows,
  * tokio workers, grpc/src/service.rs:49-65; recovery is
  * recover_from_da_slice). zg_submit queues a request and returns at once;
  * zg_wait blocks for its result (timeout_ms < 0: no limit; ZG_ERR_TIMEOUT
- * leaves it queued). Requests run in submission order; two blob slots let one
- * blob's host<->device copies overlap another's compute. The caller keeps
- * the request's input buffers valid until zg_wait has returned its result.
- * Encode replies are zg_encode's; recovery replies hold the payload
+ * leaves it queued). Continuous batching: encode requests are taken in
+ * submission order by units, each a stream with its own device buffers for
+ * up to ZG_MAX_FUSED_BLOBS blobs; a unit takes every waiting request up to
+ * that count and encodes them as one launch sequence whose bucket
+ * accumulation spans all their MSMs, replayed from a CUDA graph. A new unit
+ * is created when every unit is busy, requests are waiting and the device's
+ * free memory covers one more unit plus the reserve, so admission follows
+ * free HBM; units run concurrently on the device (one unit's copies and
+ * small kernels beside another's MSM). Recovery requests run beside the
+ * encodes on their own stream. The caller keeps the request's input buffers
+ * valid until zg_wait has returned its result. Encode replies are
+ * zg_encode's, bit for bit; recovery replies hold the payload
  * (zg_reply_payload). A failed request's status comes back from zg_wait with
  * its message in zg_last_error(). TooLargeBlob is reported by zg_submit. */
 #define ZG_REQ_ENCODE 0
@@ -186,6 +220,28 @@ const uint8_t* zg_reply_payload(const zg_reply* r, size_t* len);
  * is returned. */
 int zg_encode_batch(zg_ctx* ctx, size_t n, const uint8_t* const* data, const size_t* lens, int require_data,
                     zg_reply** out);
+/* Pipeline settings (no reference counterpart): max_units caps the units
+ * (0 = as many as the free HBM allows, at most 8), blobs_per_launch the
+ * blobs a unit fuses into one launch sequence (0 = ZG_MAX_FUSED_BLOBS, 1 =
+ * no fusing), reserve_mib the device memory admission leaves free (0 = 4096).
+ * Takes effect for the next request: a running pipeline is drained and
+ * restarted. zg_ctx_pipeline_stats reports what the pipeline did since the
+ * context was created. */
+#define ZG_MAX_FUSED_BLOBS 2
+typedef struct zg_pipeline_config {
+  uint32_t max_units;
+  uint32_t blobs_per_launch;
+  uint32_t reserve_mib;
+} zg_pipeline_config;
+typedef struct zg_pipeline_stats {
+  uint64_t units;             /* units created */
+  uint64_t launches[ZG_MAX_FUSED_BLOBS]; /* unit launches of k + 1 blobs */
+  uint64_t max_in_flight;     /* most encode requests on the device at once */
+  uint64_t recoveries;        /* recovery requests run */
+  uint64_t unit_bytes;        /* device bytes of one unit */
+} zg_pipeline_stats;
+int zg_ctx_set_pipeline(zg_ctx* ctx, const zg_pipeline_config* cfg);
+int zg_ctx_pipeline_stats(zg_ctx* ctx, zg_pipeline_stats* out);
 
 /* One MSM over the first n points of a param line with the context's
  * fixed-base tables: out = sum_i scalars[i] * line[i], written as a 64-byte
@@ -293,7 +349,8 @@ int zg_merkle_roots(const void* d_items, size_t n_items, void* d_roots, void* st
  * field and curve routines against the host build of the same code on fixed
  * pseudo-random inputs; fails[k] receives the mismatch count of check k
  * (0 Fq mul, 1 Fq mul on the FP64 pipe, 2 Fq add, 3 Fq sub, 4 Fr mul,
- * 5 Fr Montgomery round trip, 6 XYZZ add(P, P) == dbl(P)). */
+ * 5 Fr Montgomery round trip, 6 XYZZ add(P, P) == dbl(P), 7 Fq mul with
+ * 28-bit limbs). */
 int zg_selftest(int* fails, int nops);
 
 const char* zg_last_error(void);

@@ -77,7 +77,7 @@ def test_device_arithmetic_selftest(gpu_pkg):
     FP64-pipe Fq product the MSM pairs with the integer one."""
     fails = gpu_pkg.selftest()
     assert fails == {k: 0 for k in fails}, fails
-    assert "fq_mul_f64" in fails
+    assert "fq_mul_f64" in fails and "fq_mul_w28" in fails
 
 
 @pytest.mark.parametrize("log_n,batch,inverse,coset", [
@@ -274,13 +274,15 @@ def test_encode_matches_oracle(gpu_pkg, oracle, log_row, log_col):
     params.close()
 
 
-@pytest.mark.parametrize("product,cpb,threads", [
-    ("imad", 1, 128), ("hybrid", 4, 512), ("fp64", 2, 256), ("imad", 2, 512), ("fp64", 4, 128),
+@pytest.mark.parametrize("product,cpb,threads,task", [
+    ("imad", 1, 128, 64), ("hybrid", 4, 512, 32), ("fp64", 2, 256, 48), ("imad", 2, 512, 96),
+    ("fp64", 4, 128, 64), ("w28", 1, 256, 32), ("w28_hybrid", 2, 128, 96), ("w28_hybrid", 4, 256, 64),
 ])
-def test_tuning_choices_match_oracle(gpu_pkg, oracle, product, cpb, threads):
-    """Every kernel choice the tuning can make (MSM product kind, RS column
-    tile and block size) gives the oracle's bytes, on the plain path and on
-    the request pipeline (whose CUDA graphs are re-captured on a change)."""
+def test_tuning_choices_match_oracle(gpu_pkg, oracle, product, cpb, threads, task):
+    """Every kernel choice the tuning can make (MSM product kind, bucket task
+    size, RS column tile and block size) gives the oracle's bytes, on the
+    plain path and on the request pipeline (whose CUDA graphs are re-captured
+    on a change)."""
     params = gpu_pkg.ZgEncoderParams.from_seed(5, 6, 17)
     op = oracle.params(5, 6, 17)
     payload = np.random.default_rng(cpb * threads).integers(0, 256, size=params.dims.max_raw_data_size - 3,
@@ -289,15 +291,40 @@ def test_tuning_choices_match_oracle(gpu_pkg, oracle, product, cpb, threads):
     # the pipeline first runs (and captures its graphs) with the default choice
     first = gpu_pkg.EncoderService(params).process_batch([payload], True)[0]
     assert first.storage_root == exp.file_root()
-    params.set_tuning(product, cpb, threads)
+    params.set_tuning(product, cpb, threads, msm_task=task)
     t = params.tuning()
-    assert (t["msm_product"], t["ntt_cols_per_cta"], t["ntt_threads"]) == (product, cpb, threads)
+    assert (t["msm_product"], t["ntt_cols_per_cta"], t["ntt_threads"], t["msm_task"]) == \
+        (product, cpb, threads, task)
     _check_against_oracle(gpu_pkg, oracle, params, op, payload)
     again = gpu_pkg.EncoderService(params).process_batch([payload], True)[0]
     assert again.encoded_slice == [exp.slice(i) for i in range(params.dims.rows_encoded)]
     assert again.erasure_commitment == exp.commitment()
     with pytest.raises(RuntimeError):
         params.set_tuning(product, 3, threads)
+    with pytest.raises(RuntimeError):
+        params.set_tuning(product, cpb, threads, msm_task=40)
+    params.close()
+
+
+def test_wide_class_choices_match_oracle(gpu_pkg, oracle):
+    """At 32 x 1024 the context holds five wide-window classes; every number of
+    them in use (the lines of the others on 11-bit chunk windows) gives the
+    oracle's bytes."""
+    params = gpu_pkg.ZgEncoderParams.from_seed(5, 10, 13)
+    op = oracle.params(5, 10, 13)
+    avail = params.tuning()["msm_wide_avail"]
+    assert avail == 5
+    payload = np.random.default_rng(13).integers(0, 256, size=params.dims.max_raw_data_size // 3,
+                                                 dtype=np.uint8).tobytes()
+    exp = oracle.encode(op, payload)
+    lines = []
+    for k in range(avail + 1):
+        params.set_tuning("hybrid", 2, 256, msm_task=64, msm_wide_classes=k)
+        lines.append(params.tuning()["msm_wide_lines"])
+        r = gpu_pkg.EncoderService(params).process_data(payload, False)
+        assert r.erasure_commitment == exp.commitment(), k
+        assert r.encoded_slice == [exp.slice(i) for i in range(params.dims.rows_encoded)], k
+    assert lines == sorted(lines) and lines[0] == 0 and lines[-1] == 5
     params.close()
 
 
@@ -309,9 +336,12 @@ def test_autotune_then_encode(gpu_pkg, oracle):
     t = params.autotune()
     assert t["msm_product"] in gpu_pkg.MSM_PRODUCTS
     assert all(x > 0 for x in t["msm_ms"]) and all(x > 0 for x in t["ntt_ms"])
+    assert all(x > 0 for x in t["task_ms"])
     k = gpu_pkg.MSM_PRODUCTS.index(t["msm_product"])
     assert t["msm_ms"][k] == min(t["msm_ms"])
+    assert t["task_ms"][gpu_pkg.MSM_TASK_SIZES.index(t["msm_task"])] == min(t["task_ms"])
     assert params.tuning()["msm_product"] == t["msm_product"]
+    assert params.tuning()["msm_task"] == t["msm_task"]
     payload = np.random.default_rng(5).integers(0, 256, size=4321, dtype=np.uint8).tobytes()
     _check_against_oracle(gpu_pkg, oracle, params, op, payload)
     params.close()

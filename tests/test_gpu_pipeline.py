@@ -71,3 +71,42 @@ def test_mixed_requests_match_alone(svc):
         else:
             with pytest.raises(pkg.RecoveryError, match="Not enough valid lines"):
                 s.wait(t)
+
+
+@pytest.mark.parametrize("blobs_per_launch", [2, 1])
+def test_fused_launches_match_plain(svc, blobs_per_launch):
+    """Requests waiting together are fused into one unit launch (one bucket
+    accumulation over both blobs' MSM items) when blobs_per_launch is 2, and
+    run one per launch when it is 1; every reply equals the plain path's."""
+    pkg, params, s = svc
+    params.set_pipeline(max_units=2, blobs_per_launch=blobs_per_launch)
+    before = params.pipeline_stats()
+    payloads = _payloads(params.dims.max_raw_data_size, 9, 5)
+    alone = [s.process_data(p, True) for p in payloads]
+    assert s.process_batch(payloads, True) == alone  # nine requests queued at once
+    tickets = [s.submit(p, True) for p in payloads]
+    for t, a in zip(tickets, alone):
+        assert s.wait(t) == a
+    st = params.pipeline_stats()
+    fused = st["launches_by_blobs"][2] - before["launches_by_blobs"][2]
+    if blobs_per_launch == 1:
+        assert fused == 0
+    else:
+        assert fused >= 4  # the batch's nine requests fill at least four pairs
+    assert st["max_in_flight"] >= 2
+    params.set_pipeline()
+
+
+def test_fused_launches_wide_windows(gpu_pkg):
+    """Fused pairs at 32 x 1024, where each blob's MSM is six item sets (the
+    chunk lines and five wide-window unit sizes), twelve in the shared launch."""
+    params = gpu_pkg.ZgEncoderParams.from_seed(5, 10, 9)
+    try:
+        s = gpu_pkg.EncoderService(params)
+        params.set_pipeline(max_units=1, blobs_per_launch=2)
+        payloads = _payloads(params.dims.max_raw_data_size, 4, 6)
+        alone = [s.process_data(p, False) for p in payloads]
+        assert s.process_batch(payloads, False) == alone
+        assert params.pipeline_stats()["launches_by_blobs"][2] >= 2
+    finally:
+        params.close()
