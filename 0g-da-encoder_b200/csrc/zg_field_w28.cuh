@@ -1,4 +1,4 @@
-// BN254 Fq Montgomery product with 28-bit limbs and 64-bit column sums.
+// BN254 Montgomery product (Fq or Fr) with 28-bit limbs and 64-bit column sums.
 //
 // Fq::mul runs the 8 x 32-bit CIOS rows as carry chains (mad.lo.cc /
 // madc.hi.cc): every step waits on the previous one's carry flag, and on
@@ -26,17 +26,30 @@ namespace zg {
 namespace w28 {
 
 constexpr uint32_t M28 = (1u << 28) - 1;
-constexpr uint32_t PINV28 = 0x4866389u;  // -p^-1 mod 2^28
-constexpr uint32_t PINV4 = 0x9u;         // -p^-1 mod 2^4
 
-// 28-bit limb j of the Fq modulus
-ZG_HD constexpr uint32_t P(int j) {
-  return j == 0 ? 0x87cfd47u : j == 1 ? 0x208c16du : j == 2 ? 0x1ca8d3cu : j == 3 ? 0x6a91687u
-       : j == 4 ? 0x85d9781u : j == 5 ? 0xb681815u : j == 6 ? 0x9b85045u : j == 7 ? 0xe131a02u
-       : j == 8 ? 0x644e72u : 0x3u;
-}
+// 28-bit limbs of the moduli and -p^-1 mod 2^28 / mod 2^4
+struct FqLimbs {
+  static constexpr uint32_t PINV28 = 0x4866389u, PINV4 = 0x9u;
+  static ZG_HD constexpr uint32_t P(int j) {
+    return j == 0 ? 0x87cfd47u : j == 1 ? 0x208c16du : j == 2 ? 0x1ca8d3cu : j == 3 ? 0x6a91687u
+         : j == 4 ? 0x85d9781u : j == 5 ? 0xb681815u : j == 6 ? 0x9b85045u : j == 7 ? 0xe131a02u
+         : j == 8 ? 0x644e72u : 0x3u;
+  }
+};
+struct FrLimbs {
+  static constexpr uint32_t PINV28 = 0xfffffffu, PINV4 = 0xfu;
+  static ZG_HD constexpr uint32_t P(int j) {
+    return j == 0 ? 0x1u : j == 1 ? 0xe1f593fu : j == 2 ? 0x9709143u : j == 3 ? 0xe84879bu
+         : j == 4 ? 0x85d2833u : j == 5 ? 0xb681815u : j == 6 ? 0x9b85045u : j == 7 ? 0xe131a02u
+         : j == 8 ? 0x644e72u : 0x3u;
+  }
+};
+template <class C> struct Limbs;
+template <> struct Limbs<FqCfg> : FqLimbs {};
+template <> struct Limbs<FrCfg> : FrLimbs {};
 
-ZG_HD void split(const Fq& a, uint32_t x[10]) {
+template <class C>
+ZG_HD void split(const Fp<C>& a, uint32_t x[10]) {
   const uint32_t* v = a.v;
   x[0] = v[0] & M28;
   x[1] = ((v[0] >> 28) | (v[1] << 4)) & M28;
@@ -50,8 +63,10 @@ ZG_HD void split(const Fq& a, uint32_t x[10]) {
   x[9] = v[7] >> 28;
 }
 
-// a * b / 2^256 mod p for a, b < p; result < p
-ZG_HD Fq mont_mul(const Fq& a, const Fq& b) {
+// a * b / 2^256 mod p for a, b < p; result < p (p the modulus of C: Fq or Fr)
+template <class C>
+ZG_HD Fp<C> mont_mul(const Fp<C>& a, const Fp<C>& b) {
+  typedef Limbs<C> L;
   uint32_t x[10], y[10];
   split(a, x);
   split(b, y);
@@ -64,15 +79,15 @@ ZG_HD Fq mont_mul(const Fq& a, const Fq& b) {
     for (int j = 0; j < 10; ++j) t[i + j] += (uint64_t)x[i] * y[j];
 #pragma unroll
   for (int i = 0; i < 9; ++i) {
-    const uint32_t m = ((uint32_t)t[i] * PINV28) & M28;
+    const uint32_t m = ((uint32_t)t[i] * L::PINV28) & M28;
 #pragma unroll
-    for (int j = 0; j < 10; ++j) t[i + j] += (uint64_t)m * P(j);
+    for (int j = 0; j < 10; ++j) t[i + j] += (uint64_t)m * L::P(j);
     t[i + 1] += t[i] >> 28;
   }
   {
-    const uint32_t m = ((uint32_t)t[9] * PINV4) & 15u;
+    const uint32_t m = ((uint32_t)t[9] * L::PINV4) & 15u;
 #pragma unroll
-    for (int j = 0; j < 10; ++j) t[9 + j] += (uint64_t)m * P(j);
+    for (int j = 0; j < 10; ++j) t[9 + j] += (uint64_t)m * L::P(j);
   }
   // columns 9.. into 28-bit limbs r[0..9] (value r * 2^252, r[0] % 16 == 0)
   uint32_t r[10];
@@ -84,7 +99,7 @@ ZG_HD Fq mont_mul(const Fq& a, const Fq& b) {
     c >>= 28;
   }
   // drop the 4 low bits: bit 28 k - 4 of the result is bit 0 of r[k]
-  Fq o;
+  Fp<C> o;
   o.v[0] = (r[0] >> 4) | (r[1] << 24);
   o.v[1] = (r[1] >> 8) | (r[2] << 20);
   o.v[2] = (r[2] >> 12) | (r[3] << 16);
@@ -93,8 +108,8 @@ ZG_HD Fq mont_mul(const Fq& a, const Fq& b) {
   o.v[5] = (r[5] >> 24) | (r[6] << 4);
   o.v[6] = r[7] | (r[8] << 28);
   o.v[7] = (r[8] >> 4) | (r[9] << 24);
-  Fq s;
-  const uint32_t borrow = Fq::sub_raw(s, o, Fq::modulus());
+  Fp<C> s;
+  const uint32_t borrow = Fp<C>::sub_raw(s, o, Fp<C>::modulus());
   return borrow ? o : s;
 }
 

@@ -26,21 +26,76 @@ __device__ __forceinline__ uint32_t brev_bits(uint32_t x, int bits) {
 }
 
 // ---------------------------------------------------------------------------
-// shared-memory radix-2 DIT NTT; s[] holds the input in bit-reversed order,
-// tw[k] = w^k for k < n/2 of the n-th root in use. Result in natural order.
-__device__ __forceinline__ void ntt_smem(Fr* s, int logn, const Fr* __restrict__ tw) {
+// Shared-memory DIT NTT in radix-2^3 passes; s[] holds the input in
+// bit-reversed order, tw[k] = w^k for k < n/2 of the n-th root in use. Result
+// in natural order. Stage st pairs elements half = 2^(st-1) apart with
+// twiddle w^((n >> st) * (i mod half)). A pass runs three stages st .. st + 2
+// in registers: each thread takes the eight elements base + j h (h = 2^(st-1),
+// base with bits st-1 .. st+1 clear), so the pass reads and writes shared
+// memory once instead of three times and needs one barrier instead of three.
+// One or two leftover stages run as a radix-2 or radix-4 pass the same way.
+template <class F>
+__device__ __forceinline__ void ntt_bfly(F& a, F& b, const F& w) {
+  const F v = b * w;
+  b = a - v;
+  a = a + v;
+}
+
+template <class F>
+__device__ __forceinline__ void ntt_smem(F* s, int logn, const F* __restrict__ tw) {
   const int n = 1 << logn;
-  for (int st = 1; st <= logn; ++st) {
-    const int half = 1 << (st - 1);
-    const int stride = n >> st;
-    for (int bf = threadIdx.x; bf < (n >> 1); bf += blockDim.x) {
-      int k = bf & (half - 1);
-      int i = ((bf >> (st - 1)) << st) + k;
-      Fr w = tw[k * stride];
-      Fr u = s[i];
-      Fr v = s[i + half] * w;
-      s[i] = u + v;
-      s[i + half] = u - v;
+  int st = 1;
+  for (; st + 2 <= logn; st += 3) {
+    const int h = 1 << (st - 1);
+    const int s1 = n >> st, s2 = n >> (st + 1), s3 = n >> (st + 2);
+    for (int g = threadIdx.x; g < (n >> 3); g += blockDim.x) {
+      const int k0 = g & (h - 1);
+      const int base = ((g >> (st - 1)) << (st + 2)) + k0;
+      F x[8];
+#pragma unroll
+      for (int j = 0; j < 8; ++j) x[j] = s[base + j * h];
+      const F w1 = tw[k0 * s1];
+#pragma unroll
+      for (int j = 0; j < 8; j += 2) ntt_bfly(x[j], x[j + 1], w1);
+      const F w2a = tw[k0 * s2], w2b = tw[(k0 + h) * s2];
+      ntt_bfly(x[0], x[2], w2a);
+      ntt_bfly(x[1], x[3], w2b);
+      ntt_bfly(x[4], x[6], w2a);
+      ntt_bfly(x[5], x[7], w2b);
+#pragma unroll
+      for (int j = 0; j < 4; ++j) ntt_bfly(x[j], x[j + 4], tw[(k0 + j * h) * s3]);
+#pragma unroll
+      for (int j = 0; j < 8; ++j) s[base + j * h] = x[j];
+    }
+    __syncthreads();
+  }
+  if (st + 1 == logn) {  // two stages left: radix-4
+    const int h = 1 << (st - 1);
+    const int s1 = n >> st, s2 = n >> (st + 1);
+    for (int g = threadIdx.x; g < (n >> 2); g += blockDim.x) {
+      const int k0 = g & (h - 1);
+      const int base = ((g >> (st - 1)) << (st + 1)) + k0;
+      F x[4];
+#pragma unroll
+      for (int j = 0; j < 4; ++j) x[j] = s[base + j * h];
+      const F w1 = tw[k0 * s1];
+      ntt_bfly(x[0], x[1], w1);
+      ntt_bfly(x[2], x[3], w1);
+      ntt_bfly(x[0], x[2], tw[k0 * s2]);
+      ntt_bfly(x[1], x[3], tw[(k0 + h) * s2]);
+#pragma unroll
+      for (int j = 0; j < 4; ++j) s[base + j * h] = x[j];
+    }
+    __syncthreads();
+  } else if (st == logn) {  // one stage left: radix-2
+    const int h = 1 << (st - 1);
+    for (int g = threadIdx.x; g < (n >> 1); g += blockDim.x) {
+      const int k0 = g & (h - 1);
+      const int i = ((g >> (st - 1)) << st) + k0;
+      F a = s[i], b = s[i + h];
+      ntt_bfly(a, b, tw[k0]);
+      s[i] = a;
+      s[i + h] = b;
     }
     __syncthreads();
   }

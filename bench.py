@@ -74,20 +74,32 @@ CONFIG = {
 }
 
 
-def executed_mixed_adds(lr, lc):
+def executed_mixed_adds(lr, lc, wide_classes=5):
     """Bucket additions of table points this build runs per blob (random
     scalars): the lines whose nodes are single chunks use 24 windows per
-    point; with 1024 columns every other line uses units of 2^min(15, log2
-    node) points and floor(254 / c) + 1 windows of c = log2 unit + 1 bits."""
+    point; with 1024 columns every other line uses units of 2^u points, u =
+    min(15, log2 node), and floor(254 / c) + 1 windows of c = u + 1 bits, when
+    its class (index 15 - u, largest unit first) is among the first
+    `wide_classes` in use, else 11-bit windows per chunk."""
     n, total = 1 << (lr + lc), 0
     for line in range(lr + 2):
         node = n if line == lr + 1 else (1 << lc if line == lr else n >> (line + 1))
-        if lc == 10 and node > 1024:
-            u = min(15, node.bit_length() - 1)
+        u = min(15, node.bit_length() - 1)
+        if lc == 10 and node > 1024 and 15 - u < wide_classes:
             total += 3 * n * (254 // (u + 1) + 1)
         else:
             total += 3 * n * 24
     return total
+
+
+def executed_full_adds(lr, lc):
+    """XYZZ + XYZZ additions of the bucket reductions per blob: per MSM work
+    item (3 x lines x rows of them, 1024 buckets each) the running sums of
+    its 128 threads (two per bucket; the merges of a bucket's extra task
+    partials are not counted) and the combine of the 128 (T, S) partials
+    (2 x 127 additions plus 3 doublings)."""
+    items = 3 * (lr + 2) * (1 << lr)
+    return items * (2 * 1024 + 2 * 127 + 3)
 
 
 def set_dims(lr, lc):
@@ -762,15 +774,23 @@ def main():
     hbm, hbm_tag = measured_peaks()
     t_msm = phases["msm"] / 1000.0
     achieved = MSM_IMAD / t_msm / 1e9
+    wide_on = tuning.get("msm_wide_classes", 5)
+    ex_mixed = executed_mixed_adds(LOG_ROW, LOG_COL, wide_on)
+    ex_full = executed_full_adds(LOG_ROW, LOG_COL)
+    ex_imad = (ex_mixed * 10 + ex_full * 14) * 264
     roofline = {
         "kernel": "k_fb_accum", "bound": "imad", "achieved": achieved, "peak": imad, "unit": "G IMAD/s",
         "frac": achieved / imad, "traffic": profile_traffic(),
         "note": "work = 1509949440 mixed adds/blob x 10 Fq mul x 264 IMAD (reference decomposition; "
-                f"this build executes {executed_mixed_adds(LOG_ROW, LOG_COL)} table-point additions plus "
+                f"this build executes {ex_mixed} table-point additions plus "
                 "the bucket reductions, half of the products on the FP64 pipe, so frac may exceed 1); "
                 "peak = live mad.lo.u32 probe on this GPU (of measured); traffic = dram bytes per launch "
                 "from the committed ncu summary",
-        "executed_mixed_adds": executed_mixed_adds(LOG_ROW, LOG_COL),
+        "executed_mixed_adds": ex_mixed, "executed_full_adds": ex_full,
+        "executed_frac": ex_imad / t_msm / 1e9 / imad,
+        "executed_note": "the additions this build runs (mixed x 10 Fq products + XYZZ x 14) x 264 IMAD per "
+                         "product / MSM phase time / the live IMAD probe: a utilisation of the integer pipe as if "
+                         "every product ran there (the FP64-pipe share of the hybrid kinds counts as IMAD work)",
     }
     phase_roofs = {
         "rs_extension": {"bound": "hbm", "bytes": RS_BYTES, "ms": phases["rs"],
