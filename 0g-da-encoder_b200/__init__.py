@@ -155,6 +155,7 @@ _SIGS = {
     "zg_ctx_phase_times": (ctypes.c_int, [_P, ctypes.POINTER(ctypes.c_float), ctypes.c_int]),
     "zg_ctx_launches": (ctypes.c_uint64, [_P]),
     "zg_probe_imad": (ctypes.c_int, [ctypes.c_int, ctypes.POINTER(ctypes.c_double)]),
+    "zg_probe_products": (ctypes.c_int, [ctypes.c_int, ctypes.c_uint32, ctypes.POINTER(ctypes.c_double)]),
     "zg_recover": (ctypes.c_int, [_P, ctypes.POINTER(ctypes.c_uint64), ctypes.POINTER(ctypes.c_char_p),
                                   ctypes.POINTER(_SZ), _SZ, ctypes.c_char_p, _SZ, ctypes.POINTER(_SZ)]),
     "zg_msm_chunks": (ctypes.c_int, [_P, _P, ctypes.c_uint32, ctypes.c_uint32, ctypes.c_uint32, _P, _P]),
@@ -241,6 +242,14 @@ def probe_imad(device=0):
     """Device integer multiply-add rate, 1e9/s."""
     v = ctypes.c_double()
     _check(lib().zg_probe_imad(device, ctypes.byref(v)))
+    return v.value
+
+
+def probe_products(device=0, kind="hybrid"):
+    """Fq products per second (1e9) of one product kind as the MSM bucket
+    loop issues them (zg_probe_products)."""
+    v = ctypes.c_double()
+    _check(lib().zg_probe_products(device, MSM_PRODUCTS.index(kind), ctypes.byref(v)))
     return v.value
 
 

@@ -777,7 +777,9 @@ def main():
     wide_on = tuning.get("msm_wide_classes", 5)
     ex_mixed = executed_mixed_adds(LOG_ROW, LOG_COL, wide_on)
     ex_full = executed_full_adds(LOG_ROW, LOG_COL)
-    ex_imad = (ex_mixed * 10 + ex_full * 14) * 264
+    ex_prod = ex_mixed * 10 + ex_full * 14
+    ex_imad = ex_prod * 264
+    prod_peak = pkg.probe_products(local, tuning.get("msm_product", "hybrid"))
     roofline = {
         "kernel": "k_fb_accum", "bound": "imad", "achieved": achieved, "peak": imad, "unit": "G IMAD/s",
         "frac": achieved / imad, "traffic": profile_traffic(),
@@ -788,6 +790,13 @@ def main():
                 "from the committed ncu summary",
         "executed_mixed_adds": ex_mixed, "executed_full_adds": ex_full,
         "executed_frac": ex_imad / t_msm / 1e9 / imad,
+        "executed_products_per_s": ex_prod / t_msm,
+        "product_peak_per_s": prod_peak * 1e9,
+        "product_frac": ex_prod / t_msm / 1e9 / prod_peak,
+        "product_note": "executed Fq products (mixed additions x 10 + XYZZ additions x 14) per second of the MSM "
+                        "phase / the live product-throughput probe of the same product kind at the bucket "
+                        "kernel's launch shape (zg_probe_products): how close the bucket loop runs to the rate "
+                        "its field products can be issued",
         "executed_note": "the additions this build runs (mixed x 10 Fq products + XYZZ x 14) x 264 IMAD per "
                          "product / MSM phase time / the live IMAD probe: a utilisation of the integer pipe as if "
                          "every product ran there (the FP64-pipe share of the hybrid kinds counts as IMAD work)",

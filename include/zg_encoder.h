@@ -168,6 +168,11 @@ uint64_t zg_ctx_launches(const zg_ctx* ctx);
 /* Integer multiply-add rate of the device (independent mad.lo.u32 chains),
  * in 1e9 per second: the denominator of the MSM roofline. */
 int zg_probe_imad(int device, double* gimad_per_s);
+/* Fq Montgomery products per second (1e9) of one product kind, issued as the
+ * MSM bucket loop issues them (one dependent chain of independent product
+ * pairs per thread, the bucket kernel's launch shape): the ceiling of the
+ * bucket accumulation's executed work. */
+int zg_probe_products(int device, uint32_t kind, double* gprod_per_s);
 
 /* recover_from_da_slice (crates/recovery/src/lib.rs:15-43): original payload
  * bytes from any >= R encoded rows. rows[i] (host memory, row_lens[i] bytes)
@@ -193,9 +198,9 @@ int zg_recover(zg_ctx* ctx, const uint64_t* row_ids, const uint8_t* const* rows,
  * accumulation spans all their MSMs, replayed from a CUDA graph. A new unit
  * is created when every unit is busy, requests are waiting and the device's
  * free memory covers one more unit plus the reserve, so admission follows
- * free HBM; units run concurrently on the device (one unit's copies and
- * small kernels beside another's MSM). Recovery requests run beside the
- * encodes on their own stream. The caller keeps the request's input buffers
+ * free HBM; the units' encodes run on the device one after another in issue
+ * order while each unit's copies overlap the others' compute. Recovery
+ * requests run beside the encodes on their own stream. The caller keeps the request's input buffers
  * valid until zg_wait has returned its result. Encode replies are
  * zg_encode's, bit for bit; recovery replies hold the payload
  * (zg_reply_payload). A failed request's status comes back from zg_wait with
@@ -221,7 +226,7 @@ const uint8_t* zg_reply_payload(const zg_reply* r, size_t* len);
 int zg_encode_batch(zg_ctx* ctx, size_t n, const uint8_t* const* data, const size_t* lens, int require_data,
                     zg_reply** out);
 /* Pipeline settings (no reference counterpart): max_units caps the units
- * (0 = as many as the free HBM allows, at most 8), blobs_per_launch the
+ * (0 = 3, as far as the free HBM allows; at most 8), blobs_per_launch the
  * blobs a unit fuses into one launch sequence (0 = ZG_MAX_FUSED_BLOBS, 1 =
  * no fusing), reserve_mib the device memory admission leaves free (0 = 4096).
  * Takes effect for the next request: a running pipeline is drained and

@@ -50,7 +50,7 @@ def device_view(ptr, n):
     torch = torch_mod()
 
     class _Cai:
-        __cuda_array_interface__ = {"shape": (n,), "typestr": "|u1", "data": (ptr, True), "version": 3}
+        __cuda_array_interface__ = {"shape": (n,), "typestr": "|u1", "data": (ptr, False), "version": 3}
 
     return torch.as_tensor(_Cai(), device="cuda")
 
