@@ -346,12 +346,16 @@ struct zg_ctx {
 };
 
 // Process-wide pool of page-locked reply buffers: pinning ~200 MB per reply
-// costs far more than the copies themselves, so freed buffers are kept (up to
-// eight per size: two pipeline slots in flight plus replies being consumed)
+// costs far more than the copies themselves, so freed buffers are kept, up
+// to 16 GiB in all (a batch of 32 full replies with encoded data is 6.6 GB;
+// with a cap of eight buffers per size, a batch that returns its replies
+// together re-pinned most of them and ran slower than one blob at a time),
 // for the next reply.
 namespace {
 std::mutex g_pin_mu;
 std::multimap<size_t, void*> g_pin_pool;
+size_t g_pin_bytes = 0;  // bytes held by the pool
+constexpr size_t kPinPoolMax = 16ull << 30;
 void* pinned_get(size_t bytes) {
   {
     std::lock_guard<std::mutex> g(g_pin_mu);
@@ -359,6 +363,7 @@ void* pinned_get(size_t bytes) {
     if (it != g_pin_pool.end()) {
       void* p = it->second;
       g_pin_pool.erase(it);
+      g_pin_bytes -= bytes;
       return p;
     }
   }
@@ -369,8 +374,12 @@ void* pinned_get(size_t bytes) {
 void pinned_put(void* p, size_t bytes) {
   if (!p) return;
   std::lock_guard<std::mutex> g(g_pin_mu);
-  if (g_pin_pool.count(bytes) < 8) g_pin_pool.emplace(bytes, p);
-  else cudaFreeHost(p);
+  if (g_pin_bytes + bytes <= kPinPoolMax) {
+    g_pin_pool.emplace(bytes, p);
+    g_pin_bytes += bytes;
+  } else {
+    cudaFreeHost(p);
+  }
 }
 }  // namespace
 
