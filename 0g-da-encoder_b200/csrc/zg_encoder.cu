@@ -696,15 +696,20 @@ int check_launch() {
   return 0;
 }
 
+// Leaves, then one launch per level down to MERKLE_TOP_MAX, then the levels
+// above in one k_merkle_top launch (off[d] = 96 (2^d - 1), the layout it
+// assumes).
 int merkle_levels(const uint8_t* items, size_t n_items, uint8_t* tree, const std::vector<uint64_t>& off,
                   int depth, cudaStream_t s) {
   const unsigned T = 128;
   size_t leaves = n_items / 8;
   k_merkle_leaves<<<nblk(leaves, T), T, 0, s>>>(items, tree + off[depth], (uint32_t)leaves);
-  for (int d = depth - 1; d >= 0; --d) {
+  const int top = std::min(depth, MERKLE_TOP_MAX);
+  for (int d = depth - 1; d >= top; --d) {
     size_t cnt = (size_t)3 << d;
     k_merkle_parents<<<nblk(cnt, T), T, 0, s>>>(tree + off[d + 1], tree + off[d], (uint32_t)cnt);
   }
+  if (top > 0) k_merkle_top<<<3, std::max(1, 1 << (top - 1)), 0, s>>>(tree, top);
   return check_launch();
 }
 
@@ -734,12 +739,15 @@ BlobBufs ctx_bufs(zg_ctx* c) {
 }
 
 // Kernel launches of an encode of nb blobs on one lane: per blob 3 RS passes,
-// leaves + tree_depth parent levels, file root, the digit sorts, trees,
+// the Merkle leaves, lower parent levels and top levels, file root, the
+// digit sorts, trees,
 // serialisation and slices; once for all of them the bucket accumulation
 // (and its counter reset) and the combine (the 8-bit path: chunks + combine
 // per blob).
 uint64_t launches_per_encode(const zg_ctx* c, int nb = 1) {
-  const uint64_t per = 3 + (uint64_t)c->tree_depth + 1 + 1 + (c->fb ? 1 + (uint64_t)c->wd_on : 2) + 1 + 1 + 1;
+  const int top = std::min(c->tree_depth, MERKLE_TOP_MAX);
+  const uint64_t merkle = 1 + (uint64_t)(c->tree_depth - top) + (top > 0 ? 1 : 0);
+  const uint64_t per = 3 + merkle + 1 + (c->fb ? 1 + (uint64_t)c->wd_on : 2) + 1 + 1 + 1;
   return per * (uint64_t)nb + (c->fb ? 2 : 0);
 }
 

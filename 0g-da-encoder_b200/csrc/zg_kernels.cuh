@@ -1140,6 +1140,40 @@ __global__ void __launch_bounds__(128) k_merkle_parents(const uint8_t* __restric
   d[0] = make_ulonglong2(out[0], out[1]);
   d[1] = make_ulonglong2(out[2], out[3]);
 }
+// The upper levels of the Merkle tree in one launch: levels top - 1 .. 0
+// from level top (at most 1024 nodes per coset), one CTA per coset subtree,
+// each level hashed from the previous one in shared memory and written out.
+// Level d holds 3 * 2^d nodes (coset c's at c 2^d ..), at byte offset
+// 96 (2^d - 1) of the tree buffer. Block size max(1, 2^(top - 1)).
+constexpr int MERKLE_TOP_MAX = 10;
+__global__ void __launch_bounds__(512) k_merkle_top(uint8_t* __restrict__ tree, int top) {
+  __shared__ uint64_t sn[(1 << MERKLE_TOP_MAX) * 4];
+  const uint32_t c = blockIdx.x, n = 1u << top;
+  const uint64_t* src = reinterpret_cast<const uint64_t*>(tree + 96 * ((1ull << top) - 1) + (size_t)c * n * 32);
+  for (uint32_t i = threadIdx.x; i < 4 * n; i += blockDim.x) sn[i] = src[i];
+  __syncthreads();
+  for (int d = top - 1; d >= 0; --d) {
+    const uint32_t cnt = 1u << d, i = threadIdx.x;
+    uint64_t out[4];
+    if (i < cnt) {
+      uint64_t in[8];
+#pragma unroll
+      for (int k = 0; k < 8; ++k) in[k] = sn[8 * i + k];
+      keccak256_64(in, out);
+    }
+    __syncthreads();
+    if (i < cnt) {
+      uint64_t* dst = reinterpret_cast<uint64_t*>(tree + 96 * ((1ull << d) - 1) + ((size_t)c * cnt + i) * 32);
+#pragma unroll
+      for (int k = 0; k < 4; ++k) {
+        sn[4 * i + k] = out[k];
+        dst[k] = out[k];
+      }
+    }
+    __syncthreads();
+  }
+}
+
 // keccak(keccak(r0 || r1) || r2)  (encoder/blob.rs:64-72)
 __global__ void k_file_root(const uint8_t* __restrict__ roots, uint8_t* __restrict__ out) {
   if (threadIdx.x != 0 || blockIdx.x != 0) return;

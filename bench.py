@@ -779,7 +779,8 @@ def main():
     ex_full = executed_full_adds(LOG_ROW, LOG_COL)
     ex_prod = ex_mixed * 10 + ex_full * 14
     ex_imad = ex_prod * 264
-    prod_peak = pkg.probe_products(local, tuning.get("msm_product", "hybrid"))
+    prod_by_kind = {k: pkg.probe_products(local, k) for k in pkg.MSM_PRODUCTS}
+    prod_peak = prod_by_kind[tuning.get("msm_product", "hybrid")]
     roofline = {
         "kernel": "k_fb_accum", "bound": "imad", "achieved": achieved, "peak": imad, "unit": "G IMAD/s",
         "frac": achieved / imad, "traffic": profile_traffic(),
@@ -793,6 +794,7 @@ def main():
         "executed_products_per_s": ex_prod / t_msm,
         "product_peak_per_s": prod_peak * 1e9,
         "product_frac": ex_prod / t_msm / 1e9 / prod_peak,
+        "product_probe_by_kind": {k: v * 1e9 for k, v in prod_by_kind.items()},
         "product_note": "executed Fq products (mixed additions x 10 + XYZZ additions x 14) per second of the MSM "
                         "phase / the live product-throughput probe of the same product kind at the bucket "
                         "kernel's launch shape (zg_probe_products): how close the bucket loop runs to the rate "
