@@ -196,16 +196,20 @@ int set_smem_limits() {
 
 inline unsigned nblk(size_t n, unsigned t) { return (unsigned)((n + t - 1) / t); }
 
+// threads of a CTA that runs one 2^logn-point transform: one per radix-4
+// group of the shared-memory passes (2^(logn - 2)), within [32, 256]
+unsigned ntt_threads(int logn) { return (unsigned)std::min(256, std::max(32, 1 << std::max(0, logn - 2))); }
+
 // natural-order N-point transform out = DFT(x) (or inverse without 1/N), via
 // the column / row passes; tmp has N elements
 // (batch vectors back to back in x, tmp and out; batch <= 65535)
 void ntt4(const Twiddles& tw, const Fr* x, Fr* tmp, Fr* out, bool inverse, cudaStream_t s, uint32_t batch = 1) {
   const int lr = tw.lr, lc = tw.lc;
   const size_t R = size_t(1) << lr, C = size_t(1) << lc;
-  k_ntt4_colpass<<<dim3((unsigned)C, batch), 256, R * sizeof(Fr), s>>>(x, tmp, lr, lc, inverse ? tw.twi_r : tw.twf_r,
+  k_ntt4_colpass<<<dim3((unsigned)C, batch), ntt_threads(lr), R * sizeof(Fr), s>>>(x, tmp, lr, lc, inverse ? tw.twi_r : tw.twf_r,
                                                                       inverse ? tw.wni_lo : tw.wn_lo,
                                                                       inverse ? tw.wni_hi : tw.wn_hi);
-  k_ntt4_rowpass<<<dim3((unsigned)R, batch), 256, C * sizeof(Fr), s>>>(tmp, out, lr, lc, inverse ? tw.twi_c : tw.twf_c);
+  k_ntt4_rowpass<<<dim3((unsigned)R, batch), ntt_threads(lc), C * sizeof(Fr), s>>>(tmp, out, lr, lc, inverse ? tw.twi_c : tw.twf_c);
 }
 
 }  // namespace
@@ -3173,7 +3177,8 @@ int zg_ntt(void* d_data, uint32_t log_n, uint32_t batch, int inverse, uint32_t c
     if (!tw) return ZG_ERR_CUDA;
     for (uint32_t b0 = 0; b0 < batch;) {
       uint32_t nb = std::min<uint32_t>(batch - b0, 65535);
-      k_ntt_small<<<nb, 256, n * sizeof(Fr), s>>>(v + (size_t)b0 * n, (int)log_n, inverse ? tw->twi_c : tw->twf_c);
+      k_ntt_small<<<nb, ntt_threads((int)log_n), n * sizeof(Fr), s>>>(v + (size_t)b0 * n, (int)log_n,
+                                                                      inverse ? tw->twi_c : tw->twf_c);
       b0 += nb;
     }
   } else {
