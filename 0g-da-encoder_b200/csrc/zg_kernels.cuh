@@ -55,11 +55,20 @@ __device__ __forceinline__ void ntt_smem(F* s, int logn, const F* __restrict__ t
       const int k0 = g & (h - 1);
       const int base = ((g >> (st - 1)) << (st + 1)) + k0;
       F x0 = s[base], x1 = s[base + h], x2 = s[base + 2 * h], x3 = s[base + 3 * h];
+      // each stage's two twiddle products are independent: one interleaved
+      // pair of carry chains (F::mul2) instead of two products in a row
       const F w1 = tw[k0 * s1];
-      ntt_bfly(x0, x1, w1);
-      ntt_bfly(x2, x3, w1);
-      ntt_bfly(x0, x2, tw[k0 * s2]);
-      ntt_bfly(x1, x3, tw[(k0 + h) * s2]);
+      F v, u;
+      F::mul2(x1, w1, x3, w1, v, u);
+      x1 = x0 - v;
+      x0 = x0 + v;
+      x3 = x2 - u;
+      x2 = x2 + u;
+      F::mul2(x2, tw[k0 * s2], x3, tw[(k0 + h) * s2], v, u);
+      x2 = x0 - v;
+      x0 = x0 + v;
+      x3 = x1 - u;
+      x1 = x1 + u;
       s[base] = x0;
       s[base + h] = x1;
       s[base + 2 * h] = x2;
