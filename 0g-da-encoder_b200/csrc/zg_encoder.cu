@@ -948,25 +948,29 @@ void launch_rs(const zg_ctx* c, const Lane& ln, const uint8_t* raw, size_t len, 
   k_rows_ntt<<<dim3((unsigned)R, 2), threads, C * sizeof(Fr), s>>>(ln.Bc, enc, lr, lc, c->tw.twf_c);
 }
 
-// The pipeline of nb blobs on one lane, launches only: every blob's RS
-// extension, Merkle tree and digit sorts, ONE bucket accumulation and ONE
-// combine over all their MSM items, then every blob's AMT trees,
-// serialisation and slices. Blob i's payload is `lens[i]` bytes at b[i].raw,
-// or *b[i].d_len bytes when `by_device_len` (graph capture).
+// The pipeline of nb blobs on one lane, launches only, in three phases:
+// PHASE_PRE every blob's RS extension, Merkle tree and digit sorts;
+// PHASE_ACC ONE bucket accumulation over all their MSM items; PHASE_POST ONE
+// combine, then every blob's AMT trees, serialisation and slices. Blob i's
+// payload is `lens[i]` bytes at b[i].raw, or *b[i].d_len bytes when
+// `by_device_len` (graph capture).
+constexpr int PHASE_PRE = 1, PHASE_ACC = 2, PHASE_POST = 4, PHASE_ALL = 7;
 int encode_launches(zg_ctx* c, const Lane& ln, const BlobBufs* b, int nb, const size_t* lens, bool by_device_len,
-                    cudaStream_t s, bool marks) {
+                    cudaStream_t s, bool marks, int phases = PHASE_ALL) {
   const int lr = c->lr, lc = c->lc;
   const size_t R = c->R, N = c->N;
   if (nb < 1 || nb > ln.cap) return fail(ZG_ERR_INTERNAL, "lane capacity exceeded");
   auto mark = [&](int k) {
     if (marks && c->profiling) cudaEventRecord(c->ev[k], s);
   };
+  int rc = 0;
+  if (phases & PHASE_PRE) {
   mark(0);
   // RS extension: rows iNTT, column passes, rows NTT
   for (int i = 0; i < nb; ++i)
     launch_rs(c, ln, b[i].raw, by_device_len ? 0 : lens[i], by_device_len ? b[i].d_len : nullptr, b[i].enc,
               c->ntt_cpb, c->ntt_threads, s);
-  int rc = check_launch();
+  rc = check_launch();
   if (rc) return rc;
   mark(1);
   // Merkle tree over the encoded data and the file root
@@ -984,9 +988,14 @@ int encode_launches(zg_ctx* c, const Lane& ln, const BlobBufs* b, int nb, const 
       for (size_t k = 0; k < (size_t)c->wd_on; ++k)
         launch_wd_sort(c->wd[k].ulog, b[i].enc, lane_wd_offs(c, ln, k, i), lane_wd_ents(c, ln, k, i), lr, lc, N, s);
     }
-    launch_fb_accum(c, ln, c->msm_product, blob_acc_plan(c, ln, nb), s);
-    mark(3);
-    launch_fb_combine(ln, blob_fb_plan(c, nb), s);
+  }
+  }  // PHASE_PRE
+  if (c->fb) {
+    if (phases & PHASE_ACC) launch_fb_accum(c, ln, c->msm_product, blob_acc_plan(c, ln, nb), s);
+    if (phases & PHASE_POST) {
+      mark(3);
+      launch_fb_combine(ln, blob_fb_plan(c, nb), s);
+    }
   } else {
     MsmChunkArgs a;
     a.scalars = b[0].enc;
@@ -999,11 +1008,14 @@ int encode_launches(zg_ctx* c, const Lane& ln, const BlobBufs* b, int nb, const 
     a.scalar_coset_stride = N;
     a.base_coset_stride = (uint64_t)c->L * c->W * N;
     a.base_line_stride = (uint64_t)c->W * N;
-    k_msm_chunks<<<dim3((unsigned)R, 3), MSM_THREADS, msm_smem_bytes(lc), s>>>(a);
-    mark(3);
-    const uint32_t nmsm = (uint32_t)(3 * c->L * R);
-    k_msm_combine<<<nblk(nmsm, 64), 64, 0, s>>>(ln.win, ln.part, nmsm);
+    if (phases & PHASE_ACC) k_msm_chunks<<<dim3((unsigned)R, 3), MSM_THREADS, msm_smem_bytes(lc), s>>>(a);
+    if (phases & PHASE_POST) {
+      mark(3);
+      const uint32_t nmsm = (uint32_t)(3 * c->L * R);
+      k_msm_combine<<<nblk(nmsm, 64), 64, 0, s>>>(ln.win, ln.part, nmsm);
+    }
   }
+  if (!(phases & PHASE_POST)) return check_launch();
   const uint32_t nn = (uint32_t)(3 * (4 * R - 2));
   for (int i = 0; i < nb; ++i) {
     XYZZ* part = ln.part + (size_t)i * 3 * c->L * R;
@@ -1252,12 +1264,12 @@ int rec_setup(zg_ctx* c) {
 // device memory) and copies the replies out, all on its stream. When every
 // unit is busy and requests wait, the issuer creates another unit if the
 // device's free memory covers it plus the reserve, up to max_units; else
-// the request waits for a unit. The units' computes run one after another
-// in issue order (each fills the GPU: 16 blobs computing side by side on 8
-// units encoded 32 uneven blobs at 5.85 blobs/s against 6.29 for one blob
-// at a time), and each unit's copies overlap the others' compute. Each unit
-// has a completion thread that finishes its replies once its copies are
-// done. Recovery requests go to a
+// the request waits for a unit. The units' bucket accumulations run one
+// after another in issue order (the persistent kernel fills the GPU: 16
+// blobs computing side by side on 8 units encoded 32 uneven blobs at 5.85
+// blobs/s against 6.29 for one blob at a time), and each unit's copies and
+// smaller phases overlap the others' work. Each unit has a completion thread
+// that finishes its replies once its copies are done. Recovery requests go to a
 // worker thread that runs zg_recover on the context's recovery stream,
 // beside the encodes.
 static_assert(ZG_MAX_FUSED_BLOBS == FB_MAX_BLOBS, "header and kernels agree on the fused blob count");
@@ -1277,9 +1289,11 @@ struct Unit {
   uint8_t* h_small[FB_MAX_BLOBS] = {};  // pinned: [0,8) length, [8,200) coset commitments,
                                         // [200,296) roots, [296,328) file root
   cudaStream_t s = nullptr;
-  cudaEvent_t ev_comp = nullptr;  // end of the unit's compute (the next unit's compute waits on it)
+  cudaEvent_t ev_comp = nullptr;  // end of the unit's accumulation (the next unit's waits on it)
   cudaEvent_t ev_out = nullptr;
-  cudaGraphExec_t graph[FB_MAX_BLOBS] = {};  // per fill level k + 1
+  // per fill level k + 1, the three phases of the encode (pre, accumulation,
+  // post) as CUDA graphs
+  cudaGraphExec_t graph[FB_MAX_BLOBS][3] = {};
   uint64_t gen[FB_MAX_BLOBS] = {};           // the context's tuning_gen at each capture
   std::vector<Request*> reqs;                // in flight (empty: free)
   bool issued = false;                       // its copies and launches are queued
@@ -1300,7 +1314,7 @@ struct Engine {
   bool use_graph = true;
   int fuse = FB_MAX_BLOBS;
   size_t max_units = 3, reserve = 4ull << 30;
-  cudaEvent_t last_comp = nullptr;  // compute of the unit issued last (issuer thread only)
+  cudaEvent_t last_comp = nullptr;  // accumulation of the unit issued last (issuer thread only)
   std::thread issuer, recoverer;
 };
 
@@ -1314,8 +1328,9 @@ void complete(Engine* e, Request* q, int status, const std::string& err) {
 
 void free_unit(Unit* u) {
   if (u->ev_out) cudaEventSynchronize(u->ev_out);
-  for (cudaGraphExec_t& g : u->graph)
-    if (g) cudaGraphExecDestroy(g);
+  for (auto& gk : u->graph)
+    for (cudaGraphExec_t& g : gk)
+      if (g) cudaGraphExecDestroy(g);
   for (int i = 0; i < FB_MAX_BLOBS; ++i) {
     BlobBufs& b = u->b[i];
     void* d[] = {b.raw, b.d_len, b.enc, b.tree, b.amt, b.slices, b.file_root};
@@ -1368,32 +1383,41 @@ Unit* make_unit(Engine* e) {
   return u.release();
 }
 
-// the CUDA graph of a unit filled with k blobs (captured on first use and
-// after a tuning change)
+// the CUDA graphs of a unit filled with k blobs, one per phase (captured on
+// first use and after a tuning change)
 int unit_graph(Engine* e, Unit* u, int k) {
   zg_ctx* c = e->c;
-  cudaGraphExec_t& gx = u->graph[k - 1];
-  if (gx && u->gen[k - 1] != c->tuning_gen) {
-    cudaGraphExecDestroy(gx);
-    gx = nullptr;
+  cudaGraphExec_t* gx = u->graph[k - 1];
+  if (gx[0] && u->gen[k - 1] != c->tuning_gen) {
+    for (int ph = 0; ph < 3; ++ph) {
+      if (gx[ph]) cudaGraphExecDestroy(gx[ph]);
+      gx[ph] = nullptr;
+    }
   }
-  if (gx || !e->use_graph) return 0;
+  if (gx[0] || !e->use_graph) return 0;
   cudaStream_t cs = nullptr;
   ZG_CK(cudaStreamCreateWithFlags(&cs, cudaStreamNonBlocking));
-  cudaGraph_t g = nullptr;
-  cudaError_t err = cudaStreamBeginCapture(cs, cudaStreamCaptureModeThreadLocal);
-  int rc = 0;
-  if (err == cudaSuccess) {
-    rc = encode_launches(c, u->lane, u->b, k, nullptr, true, cs, false);
-    err = cudaStreamEndCapture(cs, &g);
+  bool ok = true;
+  for (int ph = 0; ph < 3 && ok; ++ph) {
+    cudaGraph_t g = nullptr;
+    cudaError_t err = cudaStreamBeginCapture(cs, cudaStreamCaptureModeThreadLocal);
+    int rc = 0;
+    if (err == cudaSuccess) {
+      rc = encode_launches(c, u->lane, u->b, k, nullptr, true, cs, false, 1 << ph);
+      err = cudaStreamEndCapture(cs, &g);
+    }
+    if (err == cudaSuccess && rc == 0) err = cudaGraphInstantiate(&gx[ph], g, 0);
+    if (g) cudaGraphDestroy(g);
+    ok = err == cudaSuccess && rc == 0;
   }
-  if (err == cudaSuccess && rc == 0) err = cudaGraphInstantiate(&gx, g, 0);
   u->gen[k - 1] = c->tuning_gen;
-  if (g) cudaGraphDestroy(g);
   cudaStreamDestroy(cs);
-  if (err != cudaSuccess || rc) {  // launch the kernels one by one instead
+  if (!ok) {  // launch the kernels one by one instead
     cudaGetLastError();
-    gx = nullptr;
+    for (int ph = 0; ph < 3; ++ph) {
+      if (gx[ph]) cudaGraphExecDestroy(gx[ph]);
+      gx[ph] = nullptr;
+    }
     e->use_graph = false;
   }
   return 0;
@@ -1441,18 +1465,23 @@ int issue_unit(Engine* e, Unit* u) {
     ZG_CK(cudaMemcpyAsync(u->b[i].d_len, u->h_small[i], 8, cudaMemcpyHostToDevice, s));
     if (lens[i]) ZG_CK(cudaMemcpyAsync(u->b[i].raw, src[i], lens[i], cudaMemcpyHostToDevice, s));
   }
-  // the units' computes run one after another in issue order (each fills
-  // the GPU; run side by side they only contend for SMs and L2), while a
-  // unit's copies overlap the others' compute
-  if (e->last_comp) ZG_CK(cudaStreamWaitEvent(s, e->last_comp, 0));
-  if (u->graph[k - 1]) {
-    ZG_CK(cudaGraphLaunch(u->graph[k - 1], s));
-  } else {
-    std::lock_guard<std::mutex> g(c->mu);
-    if ((rc = encode_launches(c, u->lane, u->b, k, lens, false, s, false))) return rc;
+  // The units' bucket accumulations (the persistent kernel that fills the
+  // GPU) run one after another in issue order: run side by side they only
+  // contend for SMs and L2. A unit's copies and its pre and post phases (RS,
+  // Merkle, digit sorts; combine, trees, slices) overlap the others' work.
+  for (int ph = 0; ph < 3; ++ph) {
+    if (ph == 1 && e->last_comp) ZG_CK(cudaStreamWaitEvent(s, e->last_comp, 0));
+    if (u->graph[k - 1][ph]) {
+      ZG_CK(cudaGraphLaunch(u->graph[k - 1][ph], s));
+    } else {
+      std::lock_guard<std::mutex> g(c->mu);
+      if ((rc = encode_launches(c, u->lane, u->b, k, lens, false, s, false, 1 << ph))) return rc;
+    }
+    if (ph == 1) {
+      ZG_CK(cudaEventRecord(u->ev_comp, s));
+      e->last_comp = u->ev_comp;
+    }
   }
-  ZG_CK(cudaEventRecord(u->ev_comp, s));
-  e->last_comp = u->ev_comp;
   c->launches += launches_per_encode(c, k);
   for (int i = 0; i < k; ++i) {
     const BlobBufs& b = u->b[i];
