@@ -80,6 +80,19 @@ def test_device_arithmetic_selftest(gpu_pkg):
     assert "fq_mul_f64" in fails and "fq_mul_w28" in fails
 
 
+def test_measurement_probes(gpu_pkg):
+    """The denominators of the bench's MSM fractions: the IMAD rate and the
+    Fq product rate of every product kind are positive and physical (below
+    one product per SM clock per lane)."""
+    imad = gpu_pkg.probe_imad(0)
+    assert 1e3 < imad < 1e5  # G IMAD/s
+    for kind in gpu_pkg.MSM_PRODUCTS:
+        g = gpu_pkg.probe_products(0, kind)
+        assert 1.0 < g < imad / 100, kind  # a product is > 100 IMADs
+    out = ctypes.c_double()
+    assert gpu_pkg.lib().zg_probe_products(0, len(gpu_pkg.MSM_PRODUCTS), ctypes.byref(out)) != 0  # no such kind
+
+
 @pytest.mark.parametrize("log_n,batch,inverse,coset", [
     (5, 4, 0, 0), (5, 4, 1, 0), (5, 3, 0, 1), (10, 8, 0, 0), (10, 8, 1, 0), (10, 2, 0, 2),
     (11, 2, 1, 0), (14, 1, 0, 0), (14, 1, 1, 0), (20, 1, 0, 1), (20, 1, 1, 0),
