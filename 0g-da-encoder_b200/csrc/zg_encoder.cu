@@ -1125,24 +1125,20 @@ void keep_pool_memory() {
   cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &keep);
 }
 
-// canonical -> Montgomery, times g^(i mod 2^logn) when lo is set
-__global__ void k_canon_to_mont(Fr* v, uint64_t total, int logn, const Fr* __restrict__ lo, const Fr* __restrict__ hi,
-                                int h) {
+// x * g^(i mod 2^logn) for the coset shift: a Montgomery product with the
+// Montgomery power, so canonical x gives the canonical product
+__global__ void k_coset_shift(Fr* v, uint64_t total, int logn, const Fr* __restrict__ lo, const Fr* __restrict__ hi,
+                              int h) {
   uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= total) return;
-  Fr x = Fr::from_canonical(v[i]);
-  if (lo) {
-    const uint32_t e = (uint32_t)(i & ((1ull << logn) - 1));
-    x = x * (lo[e & ((1u << h) - 1)] * hi[e >> h]);
-  }
-  v[i] = x;
+  const uint32_t e = (uint32_t)(i & ((1ull << logn) - 1));
+  v[i] = v[i] * (lo[e & ((1u << h) - 1)] * hi[e >> h]);
 }
-__global__ void k_mont_to_canon(Fr* v, uint64_t n, Fr scale, int do_scale) {
+// x * scale (Montgomery scale: canonical in, canonical out)
+__global__ void k_scale_fr(Fr* v, uint64_t n, Fr scale) {
   uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= n) return;
-  Fr x = v[i];
-  if (do_scale) x = x * scale;
-  v[i] = x.to_canonical();
+  v[i] = v[i] * scale;
 }
 // single-CTA transform of each contiguous vector (n <= 2048)
 __global__ void __launch_bounds__(256) k_ntt_small(Fr* v, int logn, const Fr* tw) {
@@ -3197,9 +3193,11 @@ int zg_ntt(void* d_data, uint32_t log_n, uint32_t batch, int inverse, uint32_t c
   const CosetPows* cp = nullptr;
   if (coset_idx && !(cp = cached_coset_pows((int)log_n, coset_idx))) return fail(ZG_ERR_CUDA, "coset table alloc failed");
   Fr ninv = host_fr_from_u32((uint32_t)n).inverse();
+  // the transforms run on the canonical values directly (linear passes with
+  // Montgomery-form twiddles keep canonical values canonical), so only the
+  // coset shift and the inverse's 1/n remain as element-wise products
   const uint64_t total = (uint64_t)batch * n;
-  k_canon_to_mont<<<nblk(total, T), T, 0, s>>>(v, total, (int)log_n, cp ? cp->lo : nullptr, cp ? cp->hi : nullptr,
-                                               cp ? cp->h : 0);
+  if (cp) k_coset_shift<<<nblk(total, T), T, 0, s>>>(v, total, (int)log_n, cp->lo, cp->hi, cp->h);
   if (log_n <= 11) {
     const Twiddles* tw = cached_twiddles(0, (int)log_n);
     if (!tw) return ZG_ERR_CUDA;
@@ -3223,7 +3221,7 @@ int zg_ntt(void* d_data, uint32_t log_n, uint32_t batch, int inverse, uint32_t c
     }
     cudaFreeAsync(tmp, s);
   }
-  k_mont_to_canon<<<nblk(total, T), T, 0, s>>>(v, total, ninv, inverse ? 1 : 0);
+  if (inverse) k_scale_fr<<<nblk(total, T), T, 0, s>>>(v, total, ninv);
   return check_launch();
 }
 

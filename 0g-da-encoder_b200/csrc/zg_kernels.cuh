@@ -110,8 +110,15 @@ __device__ __forceinline__ Fr pow_split(const Fr* lo, const Fr* hi, uint32_t e, 
   return lo[e & ((1u << lc) - 1)] * hi[e >> lc];
 }
 
+// The three passes work on canonical values without converting them to
+// Montgomery form and back: every step is linear in the data and multiplies
+// only by constants stored in Montgomery form (twiddles, coset powers, 1/N),
+// and a Montgomery product of a canonical x with c R is the canonical x c;
+// so canonical data in gives the canonical extension out (the products a
+// conversion would cost, 3 per element of a coset, are saved).
+//
 // Pass 1: original row r -> canonical enc[0][r][*], and
-// T1[r][s] = w_N^{-s r} * sum_j v_C^{-s j} D[r][j]   (Montgomery).
+// T1[r][s] = w_N^{-s r} * sum_j v_C^{-s j} D[r][j].
 // D[r][j] is the Fr of the 31-byte chunk r*C + j of the zero-padded RawData
 // whose last four bytes hold the payload length (raw_data.rs:55-73,
 // raw_blob.rs:33-40).
@@ -152,7 +159,7 @@ __global__ void __launch_bounds__(512) k_rows_from_raw(const uint8_t* __restrict
       x.v[k] = w;
     }
     store_fr(reinterpret_cast<Fr*>(enc0) + ((size_t)r * C + j), x);
-    s[brev_bits(j, lc)] = Fr::from_canonical(x);
+    s[brev_bits(j, lc)] = x;  // canonical: the passes are linear (see below)
   }
   __syncthreads();
   ntt_smem(s, lc, twi_c);
@@ -212,7 +219,7 @@ __global__ void __launch_bounds__(512) k_rows_ntt(const Fr* __restrict__ Bc, uin
   __syncthreads();
   ntt_smem(s, lc, twf_c);
   Fr* dst = reinterpret_cast<Fr*>(enc) + ((size_t)(c + 1) * R + r) * C;
-  for (int j = threadIdx.x; j < C; j += blockDim.x) store_fr(dst + j, s[j].to_canonical());
+  for (int j = threadIdx.x; j < C; j += blockDim.x) store_fr(dst + j, s[j]);
 }
 
 // ---------------------------------------------------------------------------
