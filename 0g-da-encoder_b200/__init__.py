@@ -255,10 +255,11 @@ def probe_products(device=0, kind="hybrid"):
 
 def selftest():
     """Mismatch counts of the device arithmetic against its host build."""
-    fails = (ctypes.c_int * 8)()
-    _check(lib().zg_selftest(fails, 8))
-    return dict(zip(["fq_mul", "fq_mul_f64", "fq_add", "fq_sub", "fr_mul", "fr_roundtrip", "xyzz_dbl", "fq_mul_w28"],
-                    list(fails)))
+    names = ["fq_mul", "fq_mul_f64", "fq_add", "fq_sub", "fr_mul", "fr_roundtrip", "xyzz_dbl", "fq_mul_w28",
+             "fr_mul_f64"]
+    fails = (ctypes.c_int * len(names))()
+    _check(lib().zg_selftest(fails, len(names)))
+    return dict(zip(names, list(fails)))
 
 
 class EncoderError(Exception):

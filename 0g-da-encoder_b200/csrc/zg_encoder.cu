@@ -202,14 +202,18 @@ unsigned ntt_threads(int logn) { return (unsigned)std::min(256, std::max(32, 1 <
 
 // natural-order N-point transform out = DFT(x) (or inverse without 1/N), via
 // the column / row passes; tmp has N elements
-// (batch vectors back to back in x, tmp and out; batch <= 65535)
-void ntt4(const Twiddles& tw, const Fr* x, Fr* tmp, Fr* out, bool inverse, cudaStream_t s, uint32_t batch = 1) {
+// (batch vectors back to back in x, tmp and out; batch <= 65535). With cs_lo
+// set, input i is first multiplied by g^i = cs_lo[i mod 2^cs_h] cs_hi[i >> cs_h]
+// (coset shift); with scale set, every output by *scale.
+void ntt4(const Twiddles& tw, const Fr* x, Fr* tmp, Fr* out, bool inverse, cudaStream_t s, uint32_t batch = 1,
+          const Fr* cs_lo = nullptr, const Fr* cs_hi = nullptr, int cs_h = 0, const Fr* scale = nullptr) {
   const int lr = tw.lr, lc = tw.lc;
   const size_t R = size_t(1) << lr, C = size_t(1) << lc;
-  k_ntt4_colpass<<<dim3((unsigned)C, batch), ntt_threads(lr), R * sizeof(Fr), s>>>(x, tmp, lr, lc, inverse ? tw.twi_r : tw.twf_r,
-                                                                      inverse ? tw.wni_lo : tw.wn_lo,
-                                                                      inverse ? tw.wni_hi : tw.wn_hi);
-  k_ntt4_rowpass<<<dim3((unsigned)R, batch), ntt_threads(lc), C * sizeof(Fr), s>>>(tmp, out, lr, lc, inverse ? tw.twi_c : tw.twf_c);
+  k_ntt4_colpass<<<dim3((unsigned)C, batch), ntt_threads(lr), R * sizeof(Fr), s>>>(
+      x, tmp, lr, lc, inverse ? tw.twi_r : tw.twf_r, inverse ? tw.wni_lo : tw.wn_lo, inverse ? tw.wni_hi : tw.wn_hi,
+      cs_lo, cs_hi, cs_h);
+  k_ntt4_rowpass<<<dim3((unsigned)R, batch), ntt_threads(lc), C * sizeof(Fr), s>>>(
+      tmp, out, lr, lc, inverse ? tw.twi_c : tw.twf_c, scale != nullptr, scale ? *scale : Fr::zero());
 }
 
 }  // namespace
@@ -1077,6 +1081,7 @@ const Twiddles* cached_twiddles(int lr, int lc) {
 // g^e for e < 2^logn as lo[e & (2^h - 1)] * hi[e >> h], h = (logn + 1) / 2
 // (Montgomery form), for the coset shift of zg_ntt; one pair per (device, logn,
 // coset)
+// g^e = lo[e mod 2^h] * hi[e >> h] for e < 2^logn (h = logn: lo alone)
 struct CosetPows {
   Fr* lo = nullptr;
   Fr* hi = nullptr;
@@ -1090,7 +1095,8 @@ const CosetPows* cached_coset_pows(int logn, uint32_t coset) {
   auto it = g_coset_pows.find(key);
   if (it != g_coset_pows.end()) return &it->second;
   CosetPows p;
-  p.h = (logn + 1) / 2;
+  // one full table up to the single-CTA transform's size, else split in two
+  p.h = logn <= 11 ? logn : (logn + 1) / 2;
   const size_t nlo = size_t(1) << p.h, nhi = size_t(1) << (logn - p.h);
   const Fr gen = coset_factor(logn, coset);
   std::vector<Fr> lo(nlo), hi(nhi);
@@ -1125,59 +1131,50 @@ void keep_pool_memory() {
   cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &keep);
 }
 
-// x * g^(i mod 2^logn) for the coset shift: a Montgomery product with the
-// Montgomery power, so canonical x gives the canonical product
-__global__ void k_coset_shift(Fr* v, uint64_t total, int logn, const Fr* __restrict__ lo, const Fr* __restrict__ hi,
-                              int h) {
-  uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= total) return;
-  const uint32_t e = (uint32_t)(i & ((1ull << logn) - 1));
-  v[i] = v[i] * (lo[e & ((1u << h) - 1)] * hi[e >> h]);
-}
-// x * scale (Montgomery scale: canonical in, canonical out)
-__global__ void k_scale_fr(Fr* v, uint64_t n, Fr scale) {
-  uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= n) return;
-  v[i] = v[i] * scale;
-}
-// single-CTA transform of each contiguous vector (n <= 2048)
-__global__ void __launch_bounds__(256) k_ntt_small(Fr* v, int logn, const Fr* tw) {
+// single-CTA transform of each contiguous vector (n <= 2048). The coset
+// shift (input i times g^i, from the full table cs_lo when cs_lo is set) and
+// the inverse's 1/n (output times scale, when do_scale) are products of the
+// transform's own loads and stores: Montgomery products with Montgomery
+// constants, so canonical values stay canonical.
+__global__ void __launch_bounds__(256) k_ntt_small(Fr* v, int logn, const Fr* tw, const Fr* __restrict__ cs_lo,
+                                                   int do_scale, Fr scale) {
   extern __shared__ __align__(16) uint8_t smem[];
   Fr* s = reinterpret_cast<Fr*>(smem);
   const int n = 1 << logn;
   Fr* p = v + (size_t)blockIdx.x * n;
-  for (int i = threadIdx.x; i < n; i += blockDim.x) s[brev_bits(i, logn)] = p[i];
-  __syncthreads();
-  ntt_smem(s, logn, tw);
-  for (int i = threadIdx.x; i < n; i += blockDim.x) p[i] = s[i];
+  ntt_block(s, logn, tw, [&](int i) { return cs_lo ? p[i] * cs_lo[i] : p[i]; },
+            [&](int i, const Fr& x) { p[i] = do_scale ? x * scale : x; });
 }
 
 
 // device-vs-host arithmetic self test: out[k] counts mismatches of op k over
 // n input pairs (0 Fq mul, 1 Fq mul with immediate modulus, 2 Fq add, 3 Fq sub,
 // 4 Fr mul, 5 Fr canonical round trip, 6 XYZZ add vs doubling, 7 Fq mul with
-// 28-bit limbs)
+// 28-bit limbs, 8 Fr mul on the FP64 pipe)
+constexpr int SELFTEST_OPS = 9;
 __global__ void k_selftest(const Fq* a, const Fq* b, Fq* res, uint32_t n) {
   uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= n) return;
   Fq x = a[i], y = b[i];
-  res[8 * i + 0] = Fq::mul(x, y);
-  res[8 * i + 1] = f52::mont_mul(x, y);
-  res[8 * i + 2] = Fq::add(x, y);
-  res[8 * i + 3] = Fq::sub(x, y);
+  res[SELFTEST_OPS * i + 0] = Fq::mul(x, y);
+  res[SELFTEST_OPS * i + 1] = f52::mont_mul(x, y);
+  res[SELFTEST_OPS * i + 2] = Fq::add(x, y);
+  res[SELFTEST_OPS * i + 3] = Fq::sub(x, y);
   Fr xr = *reinterpret_cast<const Fr*>(&x), yr = *reinterpret_cast<const Fr*>(&y);
   Fr m = Fr::mul(xr, yr);
-  res[8 * i + 4] = *reinterpret_cast<Fq*>(&m);
+  res[SELFTEST_OPS * i + 4] = *reinterpret_cast<Fq*>(&m);
   Fr rt = Fr::from_canonical(xr).to_canonical();
-  res[8 * i + 5] = *reinterpret_cast<Fq*>(&rt);
+  res[SELFTEST_OPS * i + 5] = *reinterpret_cast<Fq*>(&rt);
   // P + P via add() must equal dbl(); P = (x, y) is not on the curve, the
   // formulas are still polynomial identities in the coordinates
   XYZZ p1 = XYZZ::from_affine(G1Aff{x, y});
   XYZZ d1 = p1.dbl();
   XYZZ s1 = p1;
   s1.add(p1);
-  res[8 * i + 6] = (d1.X == s1.X && d1.Y == s1.Y && d1.ZZ == s1.ZZ && d1.ZZZ == s1.ZZZ) ? Fq::one() : Fq::zero();
-  res[8 * i + 7] = w28::mont_mul(x, y);
+  res[SELFTEST_OPS * i + 6] = (d1.X == s1.X && d1.Y == s1.Y && d1.ZZ == s1.ZZ && d1.ZZZ == s1.ZZZ) ? Fq::one() : Fq::zero();
+  res[SELFTEST_OPS * i + 7] = w28::mont_mul(x, y);
+  Fr mf = f52::mont_mul(xr, yr);
+  res[SELFTEST_OPS * i + 8] = *reinterpret_cast<Fq*>(&mf);
 }
 
 
@@ -3189,22 +3186,20 @@ int zg_ntt(void* d_data, uint32_t log_n, uint32_t batch, int inverse, uint32_t c
   ZG_CK(cudaFuncSetAttribute(k_ntt_small, cudaFuncAttributeMaxDynamicSharedMemorySize, 227 * 1024));
   const size_t n = size_t(1) << log_n;
   Fr* v = (Fr*)d_data;
-  const unsigned T = 256;
   const CosetPows* cp = nullptr;
   if (coset_idx && !(cp = cached_coset_pows((int)log_n, coset_idx))) return fail(ZG_ERR_CUDA, "coset table alloc failed");
-  Fr ninv = host_fr_from_u32((uint32_t)n).inverse();
+  const Fr ninv = host_fr_from_u32((uint32_t)n).inverse();
   // the transforms run on the canonical values directly (linear passes with
-  // Montgomery-form twiddles keep canonical values canonical), so only the
-  // coset shift and the inverse's 1/n remain as element-wise products
-  const uint64_t total = (uint64_t)batch * n;
-  if (cp) k_coset_shift<<<nblk(total, T), T, 0, s>>>(v, total, (int)log_n, cp->lo, cp->hi, cp->h);
+  // Montgomery-form twiddles keep canonical values canonical); the coset
+  // shift and the inverse's 1/n are products in the transforms' first loads
+  // and last stores
   if (log_n <= 11) {
     const Twiddles* tw = cached_twiddles(0, (int)log_n);
     if (!tw) return ZG_ERR_CUDA;
     for (uint32_t b0 = 0; b0 < batch;) {
       uint32_t nb = std::min<uint32_t>(batch - b0, 65535);
-      k_ntt_small<<<nb, ntt_threads((int)log_n), n * sizeof(Fr), s>>>(v + (size_t)b0 * n, (int)log_n,
-                                                                      inverse ? tw->twi_c : tw->twf_c);
+      k_ntt_small<<<nb, ntt_threads((int)log_n), n * sizeof(Fr), s>>>(
+          v + (size_t)b0 * n, (int)log_n, inverse ? tw->twi_c : tw->twf_c, cp ? cp->lo : nullptr, inverse, ninv);
       b0 += nb;
     }
   } else {
@@ -3217,11 +3212,11 @@ int zg_ntt(void* d_data, uint32_t log_n, uint32_t batch, int inverse, uint32_t c
     ZG_CK(cudaMallocAsync(&tmp, (size_t)per * n * sizeof(Fr), s));
     for (uint32_t b0 = 0; b0 < batch; b0 += per) {
       const uint32_t nb = std::min<uint32_t>(batch - b0, per);
-      ntt4(*tw, v + (size_t)b0 * n, tmp, v + (size_t)b0 * n, inverse != 0, s, nb);
+      ntt4(*tw, v + (size_t)b0 * n, tmp, v + (size_t)b0 * n, inverse != 0, s, nb, cp ? cp->lo : nullptr,
+           cp ? cp->hi : nullptr, cp ? cp->h : 0, inverse ? &ninv : nullptr);
     }
     cudaFreeAsync(tmp, s);
   }
-  if (inverse) k_scale_fr<<<nblk(total, T), T, 0, s>>>(v, total, ninv);
   return check_launch();
 }
 
@@ -3252,18 +3247,18 @@ int zg_selftest(int* fails, int nops) {
   Fq *da = nullptr, *db = nullptr, *dr = nullptr;
   ZG_CK(cudaMalloc(&da, n * sizeof(Fq)));
   ZG_CK(cudaMalloc(&db, n * sizeof(Fq)));
-  ZG_CK(cudaMalloc(&dr, 8 * n * sizeof(Fq)));
+  ZG_CK(cudaMalloc(&dr, SELFTEST_OPS * n * sizeof(Fq)));
   ZG_CK(cudaMemcpy(da, a.data(), n * sizeof(Fq), cudaMemcpyHostToDevice));
   ZG_CK(cudaMemcpy(db, b.data(), n * sizeof(Fq), cudaMemcpyHostToDevice));
   k_selftest<<<n / 128, 128>>>(da, db, dr, n);
   ZG_CK(cudaDeviceSynchronize());
-  std::vector<Fq> r(8 * n);
-  ZG_CK(cudaMemcpy(r.data(), dr, 8 * n * sizeof(Fq), cudaMemcpyDeviceToHost));
+  std::vector<Fq> r(SELFTEST_OPS * n);
+  ZG_CK(cudaMemcpy(r.data(), dr, SELFTEST_OPS * n * sizeof(Fq), cudaMemcpyDeviceToHost));
   cudaFree(da); cudaFree(db); cudaFree(dr);
-  int cnt[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+  int cnt[SELFTEST_OPS] = {};
   for (uint32_t i = 0; i < n; ++i) {
     Fq x = a[i], y = b[i];
-    Fq e[8];
+    Fq e[SELFTEST_OPS];
     e[0] = Fq::mul(x, y);
     e[1] = e[0];
     e[2] = Fq::add(x, y);
@@ -3274,9 +3269,10 @@ int zg_selftest(int* fails, int nops) {
     e[5] = *reinterpret_cast<Fq*>(&xr);
     e[6] = Fq::one();
     e[7] = e[0];
-    for (int k = 0; k < 8; ++k) cnt[k] += (r[8 * i + k] != e[k]);
+    e[8] = e[4];
+    for (int k = 0; k < SELFTEST_OPS; ++k) cnt[k] += (r[SELFTEST_OPS * i + k] != e[k]);
   }
-  for (int k = 0; k < nops && k < 8; ++k) fails[k] = cnt[k];
+  for (int k = 0; k < nops && k < SELFTEST_OPS; ++k) fails[k] = cnt[k];
   return ZG_OK;
 }
 

@@ -44,50 +44,113 @@ __device__ __forceinline__ void ntt_bfly(F& a, F& b, const F& w) {
   a = a + v;
 }
 
+// one radix-4 pass over stages st and st + 1 of the transform in s;
+// out(i, x) receives element i of the pass's result
+template <class F, class Out>
+__device__ __forceinline__ void ntt_r4_pass(const F* s, int logn, int st, const F* __restrict__ tw, Out out) {
+  const int n = 1 << logn;
+  const int h = 1 << (st - 1);
+  const int s1 = n >> st, s2 = n >> (st + 1);
+  for (int g = threadIdx.x; g < (n >> 2); g += blockDim.x) {
+    const int k0 = g & (h - 1);
+    const int base = ((g >> (st - 1)) << (st + 1)) + k0;
+    F x0 = s[base], x1 = s[base + h], x2 = s[base + 2 * h], x3 = s[base + 3 * h];
+    // each stage's two twiddle products are independent: one interleaved
+    // pair of carry chains (F::mul2) instead of two products in a row
+    // (a pair with one product on the FP64 pipe measured slower here: 108
+    // registers against 64 halve the resident CTAs)
+    const F w1 = tw[k0 * s1];
+    F v, u;
+    F::mul2(x1, w1, x3, w1, v, u);
+    x1 = x0 - v;
+    x0 = x0 + v;
+    x3 = x2 - u;
+    x2 = x2 + u;
+    F::mul2(x2, tw[k0 * s2], x3, tw[(k0 + h) * s2], v, u);
+    out(base, x0 + v);
+    out(base + h, x1 + u);
+    out(base + 2 * h, x0 - v);
+    out(base + 3 * h, x1 - u);
+  }
+  __syncthreads();
+}
+
+// the last stage alone (odd logn): radix-2
+template <class F, class Out>
+__device__ __forceinline__ void ntt_r2_pass(const F* s, int logn, const F* __restrict__ tw, Out out) {
+  const int h = 1 << (logn - 1);
+  for (int g = threadIdx.x; g < h; g += blockDim.x) {
+    F a = s[g], b = s[g + h];
+    ntt_bfly(a, b, tw[g]);
+    out(g, a);
+    out(g + h, b);
+  }
+  __syncthreads();
+}
+
+// In-place transform of s[] (input in bit-reversed order).
 template <class F>
 __device__ __forceinline__ void ntt_smem(F* s, int logn, const F* __restrict__ tw) {
-  const int n = 1 << logn;
+  auto to_s = [s](int i, const F& x) { s[i] = x; };
   int st = 1;
-  for (; st + 1 <= logn; st += 2) {
-    const int h = 1 << (st - 1);
-    const int s1 = n >> st, s2 = n >> (st + 1);
-    for (int g = threadIdx.x; g < (n >> 2); g += blockDim.x) {
-      const int k0 = g & (h - 1);
-      const int base = ((g >> (st - 1)) << (st + 1)) + k0;
-      F x0 = s[base], x1 = s[base + h], x2 = s[base + 2 * h], x3 = s[base + 3 * h];
-      // each stage's two twiddle products are independent: one interleaved
-      // pair of carry chains (F::mul2) instead of two products in a row
-      const F w1 = tw[k0 * s1];
-      F v, u;
-      F::mul2(x1, w1, x3, w1, v, u);
-      x1 = x0 - v;
-      x0 = x0 + v;
-      x3 = x2 - u;
-      x2 = x2 + u;
-      F::mul2(x2, tw[k0 * s2], x3, tw[(k0 + h) * s2], v, u);
-      x2 = x0 - v;
-      x0 = x0 + v;
-      x3 = x1 - u;
-      x1 = x1 + u;
-      s[base] = x0;
-      s[base + h] = x1;
-      s[base + 2 * h] = x2;
-      s[base + 3 * h] = x3;
+  for (; st + 1 <= logn; st += 2) ntt_r4_pass(s, logn, st, tw, to_s);
+  if (st == logn) ntt_r2_pass(s, logn, tw, to_s);
+}
+
+// Transform of n = 2^logn elements with its input and output fused into the
+// first and last passes: element i of the natural-order input is get(i)
+// (called once per element), element k of the result goes to put(k, x)
+// (once per element); s[] is n elements of scratch that neither get nor put
+// may touch. The first pass reads its four inputs straight from get: the
+// group at bit-reversed positions 4g .. 4g+3 holds the natural elements
+// t, t + n/2, t + n/4, t + 3n/4 for g = bitrev(t), so thread t loads them
+// (coalesced across threads) and runs stages 1 and 2 in registers, whose
+// twiddles are 1 except w^(n/4): one product instead of four, and no pass of
+// its own over shared memory. The last pass writes its results to put instead
+// of back to s. Ends with a barrier.
+template <class F, class Get, class Put>
+__device__ __forceinline__ void ntt_block(F* s, int logn, const F* __restrict__ tw, Get get, Put put) {
+  if (logn < 2) {
+    if (threadIdx.x == 0) {
+      F a = get(0);
+      if (logn == 1) {
+        F b = get(1);
+        ntt_bfly(a, b, tw[0]);
+        put(1, b);
+      }
+      put(0, a);
     }
     __syncthreads();
+    return;
   }
-  if (st == logn) {  // one stage left: radix-2
-    const int h = 1 << (st - 1);
-    for (int g = threadIdx.x; g < (n >> 1); g += blockDim.x) {
-      const int k0 = g & (h - 1);
-      const int i = ((g >> (st - 1)) << st) + k0;
-      F a = s[i], b = s[i + h];
-      ntt_bfly(a, b, tw[k0]);
-      s[i] = a;
-      s[i + h] = b;
+  const int q = 1 << (logn - 2);
+  const F wq = tw[q];
+  for (int t = threadIdx.x; t < q; t += blockDim.x) {
+    const F x0 = get(t), x1 = get(t + 2 * q), x2 = get(t + q), x3 = get(t + 3 * q);
+    const F y0 = x0 + x1, y1 = x0 - x1, y2 = x2 + x3;
+    const F u = (x2 - x3) * wq;
+    if (logn == 2) {
+      put(0, y0 + y2);
+      put(1, y1 + u);
+      put(2, y0 - y2);
+      put(3, y1 - u);
+    } else {
+      const int b = (int)brev_bits(t, logn - 2) << 2;
+      s[b] = y0 + y2;
+      s[b + 1] = y1 + u;
+      s[b + 2] = y0 - y2;
+      s[b + 3] = y1 - u;
     }
-    __syncthreads();
   }
+  __syncthreads();
+  if (logn == 2) return;
+  auto to_s = [s](int i, const F& x) { s[i] = x; };
+  int st = 3;
+  for (; st + 2 <= logn; st += 2) ntt_r4_pass(s, logn, st, tw, to_s);
+  if (st + 1 == logn)
+    ntt_r4_pass(s, logn, st, tw, put);
+  else
+    ntt_r2_pass(s, logn, tw, put);
 }
 
 __device__ __forceinline__ Fr load_fr(const Fr* p) {
@@ -145,7 +208,9 @@ __global__ void __launch_bounds__(512) k_rows_from_raw(const uint8_t* __restrict
     bytes[i] = v;
   }
   __syncthreads();
-  for (int j = threadIdx.x; j < C; j += blockDim.x) {
+  // element j: unpacked once, stored to enc0 (canonical: the passes are
+  // linear, see above) and handed to the transform
+  auto get = [&](int j) {
     Fr x;
     const uint8_t* b = bytes + 31 * j;
 #pragma unroll
@@ -159,15 +224,15 @@ __global__ void __launch_bounds__(512) k_rows_from_raw(const uint8_t* __restrict
       x.v[k] = w;
     }
     store_fr(reinterpret_cast<Fr*>(enc0) + ((size_t)r * C + j), x);
-    s[brev_bits(j, lc)] = x;  // canonical: the passes are linear (see below)
-  }
-  __syncthreads();
-  ntt_smem(s, lc, twi_c);
+    return x;
+  };
+  // the result stays in s and takes its twiddles in a loop of its own (in
+  // the last pass the table loads and two products per element raise the
+  // registers past three resident CTAs)
+  ntt_block(s, lc, twi_c, get, [&](int k, const Fr& x) { s[k] = x; });
   const uint32_t nmask = (1u << (lr + lc)) - 1;
-  for (int k = threadIdx.x; k < C; k += blockDim.x) {
-    Fr t = s[k] * pow_split(wni_lo, wni_hi, (uint32_t)k * r, lc, nmask);
-    store_fr(T1 + (size_t)r * C + k, t);
-  }
+  for (int k = threadIdx.x; k < C; k += blockDim.x)
+    store_fr(T1 + (size_t)r * C + k, s[k] * pow_split(wni_lo, wni_hi, (uint32_t)k * r, lc, nmask));
 }
 
 // Pass 2: per column s, iNTT over rows (size R), then per extension coset
@@ -187,20 +252,16 @@ __global__ void __launch_bounds__(512) k_cols(const Fr* __restrict__ T1, Fr* __r
   for (int cc = 0; cc < cpb; ++cc) {
     const uint32_t s = blockIdx.x * cpb + cc;
     if (s >= (uint32_t)C) break;
-    for (int r = threadIdx.x; r < R; r += blockDim.x)
-      coef[brev_bits(r, lr)] = load_fr(T1 + (size_t)r * C + s);
-    __syncthreads();
-    ntt_smem(coef, lr, twi_r);
+    // coefficients of column s (in place in coef, its own scratch: the last
+    // pass writes each element where it read it)
+    ntt_block(coef, lr, twi_r, [&](int r) { return load_fr(T1 + (size_t)r * C + s); },
+              [&](int k, const Fr& x) { coef[k] = x; });
     for (int c = 0; c < 2; ++c) {
       const Fr glo = gs_lo[c * C + s];
-      for (int q = threadIdx.x; q < R; q += blockDim.x)
-        work[brev_bits(q, lr)] = coef[q] * glo * gs_hi[c * R + q];
-      __syncthreads();
-      ntt_smem(work, lr, twf_r);
-      for (int r = threadIdx.x; r < R; r += blockDim.x) {
-        Fr t = work[r] * pow_split(wn_lo, wn_hi, s * (uint32_t)r, lc, nmask);
-        store_fr(Bc + ((size_t)c * R + r) * C + s, t);
-      }
+      ntt_block(work, lr, twf_r, [&](int q) { return coef[q] * glo * gs_hi[c * R + q]; },
+                [&](int r, const Fr& x) { work[r] = x; });
+      for (int r = threadIdx.x; r < R; r += blockDim.x)
+        store_fr(Bc + ((size_t)c * R + r) * C + s, work[r] * pow_split(wn_lo, wn_hi, s * (uint32_t)r, lc, nmask));
       __syncthreads();
     }
   }
@@ -215,11 +276,8 @@ __global__ void __launch_bounds__(512) k_rows_ntt(const Fr* __restrict__ Bc, uin
   const uint32_t r = blockIdx.x, c = blockIdx.y;
   Fr* s = reinterpret_cast<Fr*>(smem);
   const Fr* src = Bc + ((size_t)c * R + r) * C;
-  for (int k = threadIdx.x; k < C; k += blockDim.x) s[brev_bits(k, lc)] = load_fr(src + k);
-  __syncthreads();
-  ntt_smem(s, lc, twf_c);
   Fr* dst = reinterpret_cast<Fr*>(enc) + ((size_t)(c + 1) * R + r) * C;
-  for (int j = threadIdx.x; j < C; j += blockDim.x) store_fr(dst + j, s[j]);
+  ntt_block(s, lc, twf_c, [&](int k) { return load_fr(src + k); }, [&](int j, const Fr& x) { store_fr(dst + j, x); });
 }
 
 // ---------------------------------------------------------------------------
@@ -1297,35 +1355,40 @@ __global__ void k_quot_coeff(const Fr* pw, Fr* c, uint32_t M, uint32_t n) {
 // generic four-step NTT pass A: for each column s (C of them) of x viewed as
 // [R][C] row-major: R-point transform over q, times w_N^{s r}; writes Y[r][s].
 // blockIdx.y selects the vector of a batch (vectors of R C elements back to back).
+// With cs_lo set, element i of x is first multiplied by
+// cs_lo[i mod 2^cs_h] * cs_hi[i >> cs_h] (the coset shift).
 __global__ void __launch_bounds__(256) k_ntt4_colpass(const Fr* __restrict__ x, Fr* __restrict__ y, int lr, int lc,
                                const Fr* __restrict__ tw_r, const Fr* __restrict__ w_lo,
-                               const Fr* __restrict__ w_hi) {
+                               const Fr* __restrict__ w_hi, const Fr* __restrict__ cs_lo,
+                               const Fr* __restrict__ cs_hi, int cs_h) {
   extern __shared__ __align__(16) uint8_t smem[];
-  const int R = 1 << lr, C = 1 << lc;
+  const int C = 1 << lc;
   Fr* s = reinterpret_cast<Fr*>(smem);
   const uint32_t col = blockIdx.x;
   x += (size_t)blockIdx.y << (lr + lc);
   y += (size_t)blockIdx.y << (lr + lc);
-  for (int q = threadIdx.x; q < R; q += blockDim.x) s[brev_bits(q, lr)] = load_fr(x + (size_t)q * C + col);
-  __syncthreads();
-  ntt_smem(s, lr, tw_r);
   const uint32_t nmask = (1u << (lr + lc)) - 1;
-  for (int r = threadIdx.x; r < R; r += blockDim.x)
+  auto get = [&](int q) {
+    const uint32_t i = (uint32_t)q * C + col;
+    const Fr e = load_fr(x + i);
+    return cs_lo ? e * (cs_lo[i & ((1u << cs_h) - 1)] * cs_hi[i >> cs_h]) : e;
+  };
+  ntt_block(s, lr, tw_r, get, [&](int r, const Fr& v) { s[r] = v; });
+  for (int r = threadIdx.x; r < (1 << lr); r += blockDim.x)
     store_fr(y + (size_t)r * C + col, s[r] * pow_split(w_lo, w_hi, col * (uint32_t)r, lc, nmask));
 }
 // pass B: for each r, C-point transform over s of Y[r][*]; out[j R + r]
+// (times scale when do_scale)
 __global__ void __launch_bounds__(256) k_ntt4_rowpass(const Fr* __restrict__ y, Fr* __restrict__ out, int lr, int lc,
-                               const Fr* __restrict__ tw_c) {
+                               const Fr* __restrict__ tw_c, int do_scale, Fr scale) {
   extern __shared__ __align__(16) uint8_t smem[];
   const int R = 1 << lr, C = 1 << lc;
   Fr* s = reinterpret_cast<Fr*>(smem);
   const uint32_t r = blockIdx.x;
   y += (size_t)blockIdx.y << (lr + lc);
   out += (size_t)blockIdx.y << (lr + lc);
-  for (int k = threadIdx.x; k < C; k += blockDim.x) s[brev_bits(k, lc)] = load_fr(y + (size_t)r * C + k);
-  __syncthreads();
-  ntt_smem(s, lc, tw_c);
-  for (int j = threadIdx.x; j < C; j += blockDim.x) store_fr(out + (size_t)j * R + r, s[j]);
+  ntt_block(s, lc, tw_c, [&](int k) { return load_fr(y + (size_t)r * C + k); },
+            [&](int j, const Fr& v) { store_fr(out + (size_t)j * R + r, do_scale ? v * scale : v); });
 }
 
 // fixed-base table of G: tab[w*255 + d - 1] = d * 2^{8w} * G (XYZZ)

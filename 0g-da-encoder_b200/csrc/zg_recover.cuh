@@ -43,23 +43,20 @@ __global__ void __launch_bounds__(256) k_rec_rows(const uint8_t* __restrict__ ro
   const uint32_t id = ids[blockIdx.x];
   const uint32_t c = id >> lr, r = id & ((1u << lr) - 1);
   const Fr* src = reinterpret_cast<const Fr*>(rows) + (size_t)blockIdx.x * C;
-  for (int j = threadIdx.x; j < C; j += blockDim.x) {
+  auto get = [&](int j) {
     Fr x = load_fr(src + j);
     Fr d;
     if (!Fr::sub_raw(d, x, Fr::modulus())) {  // x >= r
       atomicOr(err, 1u);
       x = Fr::zero();
     }
-    s[brev_bits(j, lc)] = Fr::from_canonical(x);
-  }
-  __syncthreads();
-  ntt_smem(s, lc, twi_c);
+    return Fr::from_canonical(x);
+  };
   const uint32_t di = rec_domain_index(id, lr);
   const uint32_t nmask = (1u << (lr + lc)) - 1;
-  for (int k = threadIdx.x; k < C; k += blockDim.x) {
-    Fr t = s[k] * ginv[(size_t)c * C + k] * pow_split(wni_lo, wni_hi, (uint32_t)k * r, lc, nmask);
-    V[(size_t)k * M + di] = t;
-  }
+  ntt_block(s, lc, twi_c, get, [&](int k, const Fr& x) {
+    V[(size_t)k * M + di] = x * ginv[(size_t)c * C + k] * pow_split(wni_lo, wni_hi, (uint32_t)k * r, lc, nmask);
+  });
 }
 
 // zw[i] = Z(W^i) (zero at the erased points) and zinv[i] = 1 / Z(k W^i),
@@ -95,12 +92,10 @@ __global__ void __launch_bounds__(256) k_rec_cols(const Fr* __restrict__ V, Fr* 
   const uint32_t col = blockIdx.x;
   const Fr* src = V + (size_t)col * M;
   // G = P_s Z on W^i (zero at the erased points, where Z vanishes) -> coefficients
-  for (uint32_t i = threadIdx.x; i < M; i += blockDim.x) a[brev_bits(i, lm)] = load_fr(src + i) * zw[i];
-  __syncthreads();
-  ntt_smem(a, lm, twi_m);
-  // evaluate G(k W^i): coefficient j times k^j / M (the inverse transform's 1/M)
-  for (uint32_t j = threadIdx.x; j < M; j += blockDim.x) a[j] = a[j] * kpow[j];
-  __syncthreads();
+  // then evaluate G(k W^i): coefficient j times k^j / M (the inverse
+  // transform's 1/M), in place (the last pass writes where it read)
+  ntt_block(a, lm, twi_m, [&](int i) { return load_fr(src + i) * zw[i]; },
+            [&](int j, const Fr& x) { a[j] = x * kpow[j]; });
   // bit-reverse permute in place for the next DIT pass
   for (uint32_t j = threadIdx.x; j < M; j += blockDim.x) {
     uint32_t rj = brev_bits(j, lm);
@@ -138,12 +133,11 @@ __global__ void __launch_bounds__(256) k_rec_cols(const Fr* __restrict__ V, Fr* 
   // P_s at W^{4r} = w_R^r for r < R: R-point forward transform of the first R
   // coefficients (the x^N term of column 0 folds onto x^0)
   Fr* b = a + M;  // second buffer of R entries
-  for (uint32_t j = threadIdx.x; j < R; j += blockDim.x) b[brev_bits(j, lr)] = (j == 0 && col == 0) ? a[0] + a[R] : a[j];
-  __syncthreads();
-  ntt_smem(b, lr, twf_r);
   const uint32_t nmask = (1u << (lr + lc)) - 1;
-  for (uint32_t r = threadIdx.x; r < R; r += blockDim.x)
-    Wout[(size_t)r * C + col] = b[r] * pow_split(wn_lo, wn_hi, col * r, lc, nmask);
+  ntt_block(b, lr, twf_r, [&](int j) { return (j == 0 && col == 0) ? a[0] + a[R] : a[j]; },
+            [&](int r, const Fr& x) {
+              Wout[(size_t)r * C + col] = x * pow_split(wn_lo, wn_hi, col * (uint32_t)r, lc, nmask);
+            });
 }
 
 // Row r of the data: C-point NTT of Wout[r][*], canonical, packed into the
@@ -155,16 +149,13 @@ __global__ void __launch_bounds__(256) k_rec_out(const Fr* __restrict__ Win, uin
   const int C = 1 << lc;
   Fr* s = reinterpret_cast<Fr*>(smem);
   const uint32_t r = blockIdx.x;
-  for (int k = threadIdx.x; k < C; k += blockDim.x) s[brev_bits(k, lc)] = load_fr(Win + (size_t)r * C + k);
-  __syncthreads();
-  ntt_smem(s, lc, twf_c);
-  for (int j = threadIdx.x; j < C; j += blockDim.x) {
-    Fr x = s[j].to_canonical();
+  ntt_block(s, lc, twf_c, [&](int k) { return load_fr(Win + (size_t)r * C + k); }, [&](int j, const Fr& v) {
+    Fr x = v.to_canonical();
     if (x.v[7] >> 24) atomicOr(err, 4u);
     uint8_t* dst = raw + 31 * ((size_t)r * C + j);
 #pragma unroll
     for (int t = 0; t < 31; ++t) dst[t] = (uint8_t)(x.v[t >> 2] >> (8 * (t & 3)));
-  }
+  });
 }
 
 }  // namespace zg

@@ -61,7 +61,7 @@ SLICE_SIZE = 312 + 32 * (1 << LOG_COL) + 160 * LOG_ROW
 MSM_ADDS = 36864 * 40960                  # 36 864 MSMs x 1024 pts, signed 8-bit windows
 MSM_IMAD = MSM_ADDS * 10 * 264            # 10 Fq mul per mixed add, 264 32-bit IMAD per Fq mul
 RS_BYTES = 201_326_592                    # 3 transforms x (read + write 32 MiB)
-RS_FR_MULS = 41_943_040                   # Fr products of the three RS passes (counted from the kernels)
+RS_FR_MULS = 37_224_448                   # Fr products of the three RS passes (counted from the kernels)
 KECCAK_F = 1_179_645                      # 393 216 x 2 leaf permutations + 393 213 node permutations
 MERKLE_BYTES = 138_411_744                # 393 216 x 256 B leaves + 393 213 x 96 B nodes
 D2H_BYTES = 3 * R * SLICE_SIZE + 3 * N * 32 + 64 * 3 + 96 + 32
@@ -102,6 +102,14 @@ def executed_full_adds(lr, lc):
     return items * (2 * 1024 + 2 * 127 + 3)
 
 
+def ntt_muls(logn):
+    """Twiddle products of one 2^logn-point transform of the device core: the
+    first two stages (twiddles 1 and w^(n/4)) cost n/4 products, every later
+    stage n/2."""
+    n = 1 << logn
+    return logn if logn < 2 else n // 4 + (logn - 2) * n // 2
+
+
 def set_dims(lr, lc):
     """Switch the module constants to another blob shape (profiling runs)."""
     global LOG_ROW, LOG_COL, R, N, PAYLOAD, SLICE_SIZE, MSM_ADDS, MSM_IMAD, RS_BYTES, MERKLE_BYTES, D2H_BYTES, \
@@ -119,8 +127,8 @@ def set_dims(lr, lc):
     # rows pass: NTT + 2 twiddle products per element; column pass: iNTT, then
     # per coset 2 scale + NTT + 2 twiddle products; rows NTT (the passes run
     # on canonical values, with no conversion products)
-    RS_FR_MULS = R * ((C_ // 2) * lc + 2 * C_) \
-        + C_ * ((R // 2) * lr + 2 * (4 * R + (R // 2) * lr)) + 2 * R * ((C_ // 2) * lc)
+    RS_FR_MULS = R * (ntt_muls(lc) + 2 * C_) + C_ * (ntt_muls(lr) + 2 * (4 * R + ntt_muls(lr))) \
+        + 2 * R * ntt_muls(lc)
     KECCAK_F = 3 * N // 8 * 2 + 3 * N // 8 - 3
     leaves = 3 * N // 8
     MERKLE_BYTES = leaves * 256 + (leaves - 3) * 96

@@ -355,7 +355,7 @@ int zg_merkle_roots(const void* d_items, size_t n_items, void* d_roots, void* st
  * pseudo-random inputs; fails[k] receives the mismatch count of check k
  * (0 Fq mul, 1 Fq mul on the FP64 pipe, 2 Fq add, 3 Fq sub, 4 Fr mul,
  * 5 Fr Montgomery round trip, 6 XYZZ add(P, P) == dbl(P), 7 Fq mul with
- * 28-bit limbs). */
+ * 28-bit limbs, 8 Fr mul on the FP64 pipe). */
 int zg_selftest(int* fails, int nops);
 
 const char* zg_last_error(void);

@@ -1,25 +1,31 @@
-"""Exact-integer model of the FP64-pipe Fq product (csrc/zg_field_f64.cuh).
+"""Exact-integer model of the FP64-pipe product (csrc/zg_field_f64.cuh), Fq and Fr.
 
 The device routine splits every 52 x 52-bit limb product with two FMAs and
 sums the bit patterns of the halves in 64-bit integer columns. This test
 restates each step with Python integers (the FMA steps are exact by
 construction, so their integer values are what the device computes) and
-checks the result against a * b / 2^256 mod p, the value of Fq::mul, plus the
-bounds the device code relies on. The device routine itself is checked against
-Fq::mul on the GPU by zg_selftest (check 1).
+checks the result against a * b / 2^256 mod p, the value of Fp::mul, plus the
+bounds the device code relies on, for both BN254 moduli (the MSM uses it over
+Fq, the NTTs over Fr). The device routine itself is checked against Fq::mul
+and Fr::mul on the GPU by zg_selftest (checks 1 and 8).
 """
 import random
 
+import pytest
+
 import zgo
 
-P = zgo.Q_MOD
 M52 = (1 << 52) - 1
 M64 = (1 << 64) - 1
 KL = 0x4330000000000000  # bit pattern of the double 2^52
 KH = 0x4670000000000000  # bit pattern of the double 2^104
-PL = [(P >> (52 * k)) & M52 for k in range(5)]
-PINV52 = (-pow(P, -1, 1 << 52)) % (1 << 52)
-PINV48 = PINV52 & ((1 << 48) - 1)
+# the constants written in Limbs52<FqCfg> / Limbs52<FrCfg>
+DEVICE_CONSTS = {
+    zgo.Q_MOD: ([0x8C16D87CFD47, 0x916871CA8D3C2, 0x181585D97816A, 0xA029B85045B68, 0x30644E72E131],
+                0x20782E4866389, 0x782E4866389),
+    zgo.R_MOD: ([0x1F593F0000001, 0x4879B9709143E, 0x181585D2833E8, 0xA029B85045B68, 0x30644E72E131],
+                0x1F593EFFFFFFF, 0xF593EFFFFFFF),
+}
 
 
 def nprod(c):
@@ -37,7 +43,10 @@ def fma_split(a, b, bits=52):
     return (a * b) >> bits, (a * b) & ((1 << bits) - 1)
 
 
-def mont_mul_model(a, b, trace=None):
+def mont_mul_model(P, a, b, trace=None):
+    PL = [(P >> (52 * k)) & M52 for k in range(5)]
+    PINV52 = (-pow(P, -1, 1 << 52)) % (1 << 52)
+    PINV48 = PINV52 & ((1 << 48) - 1)
     A = [(a >> (52 * k)) & M52 for k in range(5)]
     B = [(b >> (52 * k)) & M52 for k in range(5)]
     t = [col_init(c) for c in range(10)]
@@ -75,7 +84,16 @@ def mont_mul_model(a, b, trace=None):
     return r - P if r >= P else r
 
 
-def test_model_matches_montgomery_product():
+@pytest.mark.parametrize("P", [zgo.Q_MOD, zgo.R_MOD])
+def test_device_constants(P):
+    limbs, pinv52, pinv48 = DEVICE_CONSTS[P]
+    assert sum(x << (52 * k) for k, x in enumerate(limbs)) == P
+    assert (P * pinv52 + 1) % (1 << 52) == 0
+    assert (P * pinv48 + 1) % (1 << 48) == 0
+
+
+@pytest.mark.parametrize("P", [zgo.Q_MOD, zgo.R_MOD])
+def test_model_matches_montgomery_product(P):
     rng = random.Random(52)
     edge = [0, 1, 2, P - 1, P - 2, (1 << 253) - 1, 1 << 200]
     pairs = [(x, y) for x in edge for y in edge]
@@ -83,6 +101,6 @@ def test_model_matches_montgomery_product():
     rinv = pow(2, -256, P)
     peak = []
     for a, b in pairs:
-        assert mont_mul_model(a, b, peak) == a * b * rinv % P
+        assert mont_mul_model(P, a, b, peak) == a * b * rinv % P
     # column sums stay far below 2^64 (the device accumulates modulo 2^64)
     assert max(peak) < 1 << 58

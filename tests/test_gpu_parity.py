@@ -74,10 +74,10 @@ def mont_lines(mont: bytes, log_row, log_col):
 # ---------------------------------------------------------------------------
 def test_device_arithmetic_selftest(gpu_pkg):
     """Device field / curve routines against their host build, incl. the
-    FP64-pipe Fq product the MSM pairs with the integer one."""
+    FP64-pipe Fq product the MSM pairs with the integer one and its Fr form."""
     fails = gpu_pkg.selftest()
     assert fails == {k: 0 for k in fails}, fails
-    assert "fq_mul_f64" in fails and "fq_mul_w28" in fails
+    assert "fq_mul_f64" in fails and "fq_mul_w28" in fails and "fr_mul_f64" in fails
 
 
 def test_measurement_probes(gpu_pkg):
