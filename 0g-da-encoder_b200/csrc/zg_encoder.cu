@@ -943,7 +943,7 @@ void launch_rs(const zg_ctx* c, const Lane& ln, const uint8_t* raw, size_t len, 
                uint32_t cpb, uint32_t threads, cudaStream_t s) {
   const int lr = c->lr, lc = c->lc;
   const size_t R = c->R, C = c->C;
-  k_rows_from_raw<<<(unsigned)R, threads, C * sizeof(Fr) + 31 * C, s>>>(raw, len, d_len, c->max_raw, lr, lc, enc,
+  k_rows_from_raw<<<(unsigned)R, threads, C * sizeof(Fr) + 31 * C + 16, s>>>(raw, len, d_len, c->max_raw, lr, lc, enc,
                                                                         ln.T1, c->tw.twi_c, c->tw.wni_lo,
                                                                         c->tw.wni_hi);
   k_cols<<<nblk(C, cpb), threads, 2 * R * sizeof(Fr), s>>>(ln.T1, ln.Bc, lr, lc, c->tw.twi_r, c->tw.twf_r,

@@ -187,7 +187,11 @@ __device__ __forceinline__ Fr pow_split(const Fr* lo, const Fr* hi, uint32_t e, 
 // raw_blob.rs:33-40).
 // The payload length is `len`, or *d_len when d_len is set (graph launches,
 // whose parameters are fixed at capture).
-__global__ void __launch_bounds__(512) k_rows_from_raw(const uint8_t* __restrict__ raw, uint64_t len,
+//
+// 80 registers per thread (a few bytes spilled): three 256-thread CTAs per
+// SM, as the shared memory allows (96 registers unbounded: two, and 5 %
+// slower).
+__global__ void __maxnreg__(80) k_rows_from_raw(const uint8_t* __restrict__ raw, uint64_t len,
                                                        const uint64_t* __restrict__ d_len, uint64_t max_raw, int lr,
                                                        int lc, uint8_t* __restrict__ enc0, Fr* __restrict__ T1,
                                                        const Fr* __restrict__ twi_c, const Fr* __restrict__ wni_lo,
@@ -200,7 +204,19 @@ __global__ void __launch_bounds__(512) k_rows_from_raw(const uint8_t* __restrict
   uint8_t* bytes = smem + (size_t)C * sizeof(Fr);
   const uint64_t base = (uint64_t)31 * r * C;
   const uint32_t nbytes = 31u * C;
-  for (uint32_t i = threadIdx.x; i < nbytes; i += blockDim.x) {
+  // the row's bytes: whole 16-byte words straight from raw while they lie
+  // inside the payload (raw and the row start 16-byte aligned), the rest
+  // (payload end, zero padding, length trailer) byte by byte
+  uint32_t done = 0;
+  if (((reinterpret_cast<uintptr_t>(raw) | base) & 15) == 0 && len > base) {
+    const uint32_t nv = (uint32_t)(min(len - base, (uint64_t)nbytes) >> 4);
+    const uint4* src = reinterpret_cast<const uint4*>(raw + base);
+    uint4* dst = reinterpret_cast<uint4*>(bytes);
+#pragma unroll 4
+    for (uint32_t i = threadIdx.x; i < nv; i += blockDim.x) dst[i] = src[i];
+    done = nv << 4;
+  }
+  for (uint32_t i = done + threadIdx.x; i < nbytes; i += blockDim.x) {
     uint64_t o = base + i;
     uint8_t v = 0;
     if (o < len) v = raw[o];
@@ -208,21 +224,21 @@ __global__ void __launch_bounds__(512) k_rows_from_raw(const uint8_t* __restrict
     bytes[i] = v;
   }
   __syncthreads();
-  // element j: unpacked once, stored to enc0 (canonical: the passes are
-  // linear, see above) and handed to the transform
+  // element j: bytes 31 j .. 31 j + 30 as eight little-endian words, cut
+  // from the nine aligned words that hold them (the buffer has 16 bytes of
+  // slack behind the last element); unpacked once, stored to enc0
+  // (canonical: the passes are linear, see above) and handed to the transform
   auto get = [&](int j) {
+    // one element's loads at a time (hoisting all four elements' 36 word
+    // loads ahead would cost a resident CTA per SM in registers)
+    asm volatile("" ::: "memory");
+    const uint32_t off = 31u * (uint32_t)j;
+    const uint32_t* w = reinterpret_cast<const uint32_t*>(bytes) + (off >> 2);
+    const uint32_t sh = (off & 3) * 8;
     Fr x;
-    const uint8_t* b = bytes + 31 * j;
 #pragma unroll
-    for (int k = 0; k < 8; ++k) {
-      uint32_t w = 0;
-#pragma unroll
-      for (int t = 0; t < 4; ++t) {
-        int idx = 4 * k + t;
-        if (idx < 31) w |= (uint32_t)b[idx] << (8 * t);
-      }
-      x.v[k] = w;
-    }
+    for (int k = 0; k < 8; ++k) x.v[k] = __funnelshift_r(w[k], w[k + 1], sh);
+    x.v[7] &= 0x00ffffffu;
     store_fr(reinterpret_cast<Fr*>(enc0) + ((size_t)r * C + j), x);
     return x;
   };
@@ -240,7 +256,9 @@ __global__ void __launch_bounds__(512) k_rows_from_raw(const uint8_t* __restrict
 // multiply by w_N^{s r}; store Bc[c-1][r][s].
 // One CTA handles `cpb` consecutive columns one after the other (a tuning
 // knob: fewer, longer CTAs against more, shorter ones).
-__global__ void __launch_bounds__(512) k_cols(const Fr* __restrict__ T1, Fr* __restrict__ Bc, int lr, int lc,
+// 80 registers per thread: three 256-thread CTAs per SM (107 unbounded: two,
+// and 4 % slower).
+__global__ void __maxnreg__(80) k_cols(const Fr* __restrict__ T1, Fr* __restrict__ Bc, int lr, int lc,
                        const Fr* __restrict__ twi_r, const Fr* __restrict__ twf_r,
                        const Fr* __restrict__ gs_lo, const Fr* __restrict__ gs_hi,
                        const Fr* __restrict__ wn_lo, const Fr* __restrict__ wn_hi, int cpb) {
