@@ -97,6 +97,10 @@ def test_measurement_probes(gpu_pkg):
     (5, 4, 0, 0), (5, 4, 1, 0), (5, 3, 0, 1), (10, 8, 0, 0), (10, 8, 1, 0), (10, 2, 0, 2),
     (11, 2, 1, 0), (14, 1, 0, 0), (14, 1, 1, 0), (20, 1, 0, 1), (20, 1, 1, 0),
     (12, 4, 0, 1), (13, 3, 1, 0), (14, 5, 0, 2),  # batched four-step passes
+    # the transform core's edge shapes: one stage, the fused first pass alone,
+    # an odd last radix-2 stage, and odd four-step splits
+    (1, 3, 0, 0), (1, 2, 1, 0), (1, 2, 0, 1), (2, 3, 0, 1), (2, 2, 1, 0), (3, 2, 0, 0), (3, 2, 1, 0),
+    (4, 2, 0, 1), (7, 3, 0, 1), (9, 2, 1, 0), (15, 2, 0, 1), (17, 1, 1, 0),
 ])
 def test_ntt_matches_oracle(gpu_pkg, oracle, log_n, batch, inverse, coset):
     rng = np.random.default_rng(log_n * 100 + batch + inverse)
