@@ -121,16 +121,27 @@ std::vector<Fr> pow_table(const Fr& x, size_t n) {
   for (size_t i = 0; i < n; ++i) { t[i] = a; a = a * x; }
   return t;
 }
+// The transform core's twiddles of the n-point transform with root w, stage
+// by stage: t[h + i] = w^(i n / (2h)) for h = 1, 2, 4, .. n/2 and i < h (the
+// twiddles of the stage whose butterflies span h), t[0] = 1.
+std::vector<Fr> stage_table(const Fr& w, size_t n) {
+  std::vector<Fr> t(std::max<size_t>(n, 1));
+  t[0] = Fr::one();
+  const std::vector<Fr> p = pow_table(w, std::max<size_t>(n / 2, 1));
+  for (size_t h = 1; h < n; h <<= 1)
+    for (size_t i = 0; i < h; ++i) t[h + i] = p[i * (n / (2 * h))];
+  return t;
+}
 int make_twiddles(int lr, int lc, Twiddles* tw) {
   tw->lr = lr;
   tw->lc = lc;
   const size_t R = size_t(1) << lr, C = size_t(1) << lc, N = R * C;
   Fr wc = fr_root(lc), wr = fr_root(lr), wn = fr_root(lr + lc);
   int rc = 0;
-  if ((rc = upload(&tw->twf_c, pow_table(wc, std::max<size_t>(C / 2, 1))))) return rc;
-  if ((rc = upload(&tw->twi_c, pow_table(wc.inverse(), std::max<size_t>(C / 2, 1))))) return rc;
-  if ((rc = upload(&tw->twf_r, pow_table(wr, std::max<size_t>(R / 2, 1))))) return rc;
-  if ((rc = upload(&tw->twi_r, pow_table(wr.inverse(), std::max<size_t>(R / 2, 1))))) return rc;
+  if ((rc = upload(&tw->twf_c, stage_table(wc, C)))) return rc;
+  if ((rc = upload(&tw->twi_c, stage_table(wc.inverse(), C)))) return rc;
+  if ((rc = upload(&tw->twf_r, stage_table(wr, R)))) return rc;
+  if ((rc = upload(&tw->twi_r, stage_table(wr.inverse(), R)))) return rc;
   if ((rc = upload(&tw->wn_lo, pow_table(wn, C)))) return rc;
   if ((rc = upload(&tw->wn_hi, pow_table(wn.pow_u64(C), R)))) return rc;
   Fr wni = wn.inverse();

@@ -27,9 +27,12 @@ __device__ __forceinline__ uint32_t brev_bits(uint32_t x, int bits) {
 
 // ---------------------------------------------------------------------------
 // Shared-memory DIT NTT in radix-4 passes; s[] holds the input in
-// bit-reversed order, tw[k] = w^k for k < n/2 of the n-th root in use. Result
-// in natural order. Stage st pairs elements half = 2^(st-1) apart with
-// twiddle w^((n >> st) * (i mod half)). A pass runs two stages st, st + 1 in
+// bit-reversed order. Result in natural order. Stage st pairs elements
+// half = 2^(st-1) apart with twiddle w^((n >> st) * (i mod half)), w the
+// n-th root in use. The twiddles are stored stage by stage: tw[half + i] =
+// w^((n >> st) * i) for i < half (tw[0] = 1, n entries in all), so the
+// threads of a warp read consecutive entries at every stage instead of
+// entries n >> st apart. A pass runs two stages st, st + 1 in
 // registers: each thread takes the four elements base + j h (h = 2^(st-1),
 // base with bits st-1 and st clear), so the pass reads and writes shared
 // memory once instead of twice and needs one barrier instead of two; n / 4
@@ -50,7 +53,6 @@ template <class F, class Out>
 __device__ __forceinline__ void ntt_r4_pass(const F* s, int logn, int st, const F* __restrict__ tw, Out out) {
   const int n = 1 << logn;
   const int h = 1 << (st - 1);
-  const int s1 = n >> st, s2 = n >> (st + 1);
   for (int g = threadIdx.x; g < (n >> 2); g += blockDim.x) {
     const int k0 = g & (h - 1);
     const int base = ((g >> (st - 1)) << (st + 1)) + k0;
@@ -59,14 +61,14 @@ __device__ __forceinline__ void ntt_r4_pass(const F* s, int logn, int st, const 
     // pair of carry chains (F::mul2) instead of two products in a row
     // (a pair with one product on the FP64 pipe measured slower here: 108
     // registers against 64 halve the resident CTAs)
-    const F w1 = tw[k0 * s1];
+    const F w1 = tw[h + k0];
     F v, u;
     F::mul2(x1, w1, x3, w1, v, u);
     x1 = x0 - v;
     x0 = x0 + v;
     x3 = x2 - u;
     x2 = x2 + u;
-    F::mul2(x2, tw[k0 * s2], x3, tw[(k0 + h) * s2], v, u);
+    F::mul2(x2, tw[2 * h + k0], x3, tw[3 * h + k0], v, u);
     out(base, x0 + v);
     out(base + h, x1 + u);
     out(base + 2 * h, x0 - v);
@@ -81,7 +83,7 @@ __device__ __forceinline__ void ntt_r2_pass(const F* s, int logn, const F* __res
   const int h = 1 << (logn - 1);
   for (int g = threadIdx.x; g < h; g += blockDim.x) {
     F a = s[g], b = s[g + h];
-    ntt_bfly(a, b, tw[g]);
+    ntt_bfly(a, b, tw[h + g]);
     out(g, a);
     out(g + h, b);
   }
@@ -115,7 +117,7 @@ __device__ __forceinline__ void ntt_block(F* s, int logn, const F* __restrict__ 
       F a = get(0);
       if (logn == 1) {
         F b = get(1);
-        ntt_bfly(a, b, tw[0]);
+        ntt_bfly(a, b, tw[1]);
         put(1, b);
       }
       put(0, a);
@@ -124,7 +126,7 @@ __device__ __forceinline__ void ntt_block(F* s, int logn, const F* __restrict__ 
     return;
   }
   const int q = 1 << (logn - 2);
-  const F wq = tw[q];
+  const F wq = tw[3];  // w^(n/4), stage 2's second twiddle
   for (int t = threadIdx.x; t < q; t += blockDim.x) {
     const F x0 = get(t), x1 = get(t + 2 * q), x2 = get(t + q), x3 = get(t + 3 * q);
     const F y0 = x0 + x1, y1 = x0 - x1, y2 = x2 + x3;

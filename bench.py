@@ -110,6 +110,23 @@ def ntt_muls(logn):
     return logn if logn < 2 else n // 4 + (logn - 2) * n // 2
 
 
+def zg_ntt_products(batch, logn, inverse, coset):
+    """Fr products of one zg_ntt call: up to 2^11 points one transform per
+    vector (coset shift 1 product per element from a full table, 1/n 1
+    product); above, the four-step split (lc = ceil(logn / 2)): column
+    transforms, 2 products per element for the twiddles between the passes,
+    row transforms (coset shift 2 products per element from split tables)."""
+    n = 1 << logn
+    if logn <= 11:
+        per = ntt_muls(logn) + (n if coset else 0) + (n if inverse else 0)
+    else:
+        lc = (logn + 1) // 2
+        lr = logn - lc
+        per = (1 << lc) * ntt_muls(lr) + 2 * n + (1 << lr) * ntt_muls(lc) \
+            + (2 * n if coset else 0) + (n if inverse else 0)
+    return batch * per
+
+
 def set_dims(lr, lc):
     """Switch the module constants to another blob shape (profiling runs)."""
     global LOG_ROW, LOG_COL, R, N, PAYLOAD, SLICE_SIZE, MSM_ADDS, MSM_IMAD, RS_BYTES, MERKLE_BYTES, D2H_BYTES, \
@@ -156,6 +173,9 @@ def parse():
                     help="kernel microbenchmarks instead of the blob benchmark: single MSMs of 2^16/2^18/2^20 "
                          "points (uniform and blob-like scalars), NTTs (1024 x 2^10, 64 x 2^14, 1 x 2^20; "
                          "forward, inverse, coset), Keccak Merkle over 3072 x 1024 x 32 B")
+    ap.add_argument("--micro-cases", default="msm,ntt,merkle",
+                    help="which microbenchmarks --micro runs (comma-separated subset of msm,ntt,merkle; without "
+                         "msm no encoder context or params are built: profiling captures of the NTT kernels)")
     ap.add_argument("--tuning", default="",
                     help="PRODUCT,COLS,THREADS[,TASK[,WIDE_CLASSES]] (e.g. hybrid,1,256,64,5): use these kernel "
                          "choices instead of autotuning "
@@ -473,7 +493,8 @@ def micro(args):
     import torch
     pkg = load_pkg()
     L = pkg.lib()
-    params = pkg.ZgEncoderParams.from_seed(LOG_ROW, LOG_COL, PARAM_SEED)
+    cases = set(args.micro_cases.split(","))
+    params = pkg.ZgEncoderParams.from_seed(LOG_ROW, LOG_COL, PARAM_SEED) if "msm" in cases else None
     stream = torch.cuda.Stream()
     torch.cuda.set_stream(stream)
     flush = torch.empty(256 << 20, dtype=torch.uint8, device="cuda")
@@ -503,7 +524,7 @@ def micro(args):
     d_out = torch.empty(64, dtype=torch.uint8, device="cuda")
     basis_line = LOG_ROW  # lines: quotients 0..LOG_ROW-1, basis, high basis
     rng = np.random.default_rng(3)
-    for logn in (16, 18, 20):
+    for logn in ((16, 18, 20) if "msm" in cases else ()):
         n = 1 << logn
         for kind in ("uniform", "blob"):
             sc = rand_bytes(32 * n).view(n, 32)
@@ -525,7 +546,8 @@ def micro(args):
             nz = int((1 - z) * n) if kind == "blob" else n
             out["msm"].append({"points": n, "scalars": kind, "zero_fraction": round(z, 3), "ms": ms,
                                "points_per_s": n / (ms / 1000.0), "nonzero_points_per_s": nz / (ms / 1000.0)})
-    for batch, logn in ((1024, 10), (64, 14), (1, 20)):
+    fr_probe = pkg.probe_products(0, "imad") * 1e9 if "ntt" in cases else 0.0  # G/s -> /s
+    for batch, logn in (((1024, 10), (64, 14), (1, 20)) if "ntt" in cases else ()):
         n = 1 << logn
         for mode, inv, coset in (("forward", 0, 0), ("inverse", 1, 0), ("coset1", 0, 1)):
             v = rand_bytes(32 * n * batch).view(n * batch, 32)
@@ -538,10 +560,20 @@ def micro(args):
 
             ms = timed(run)
             byts = 2 * n * batch * 32
+            prods = zg_ntt_products(batch, logn, inv, coset)
             out["ntt"].append({"batch": batch, "log_n": logn, "mode": mode, "ms": ms,
                                "algorithmic_bytes": byts, "achieved_gbs": byts / (ms / 1000) / 1e9,
                                "hbm_frac": byts / (ms / 1000) / 1e9 / hbm,
-                               "butterfly_mul_per_s": batch * (n // 2) * logn / (ms / 1000)})
+                               "butterfly_mul_per_s": batch * (n // 2) * logn / (ms / 1000),
+                               "fr_products": prods, "fr_products_per_s": prods / (ms / 1000),
+                               "product_frac": prods / (ms / 1000) / fr_probe})
+    if "merkle" not in cases:
+        res = {"micro": out, "fr_product_probe_per_s": fr_probe, "hbm_peak_gbs": hbm, "hbm_peak_src": hbm_tag,
+               "timing": f"median of {steps} calls, CUDA events on the launching stream, L2 flushed between calls"}
+        print(json.dumps(res), flush=True)
+        if params:
+            params.close()
+        return
     items = rand_bytes(3 * N * 32)
     roots = torch.empty(96, dtype=torch.uint8, device="cuda")
 
@@ -556,11 +588,13 @@ def micro(args):
                             "achieved_gbs": MERKLE_BYTES / (ms / 1000) / 1e9,
                             "hbm_frac": MERKLE_BYTES / (ms / 1000) / 1e9 / hbm,
                             "keccak_f_per_s": (3 * N // 8 * 2 + 3 * N // 8 - 3) / (ms / 1000)}
-    res = {"micro": out, "imad_probe_gimad_s": pkg.probe_imad(0), "hbm_peak_gbs": hbm, "hbm_peak_src": hbm_tag,
+    res = {"micro": out, "imad_probe_gimad_s": pkg.probe_imad(0), "fr_product_probe_per_s": fr_probe,
+           "hbm_peak_gbs": hbm, "hbm_peak_src": hbm_tag,
            "timing": f"median of {steps} calls, CUDA events on the launching stream, L2 flushed between calls",
            "params": "seeded tau (seed 2024), 1024 x 1024, MSM bases = coset-0 basis line"}
     print(json.dumps(res), flush=True)
-    params.close()
+    if params:
+        params.close()
 
 
 def main():
