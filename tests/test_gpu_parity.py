@@ -116,6 +116,22 @@ def test_ntt_matches_oracle(gpu_pkg, oracle, log_n, batch, inverse, coset):
         assert got[b * n * 32:(b + 1) * n * 32] == exp, f"vector {b}"
 
 
+def test_ntt_large_batches_match_oracle(gpu_pkg, oracle):
+    """Batches of more vectors than the GPU holds resident CTAs (several waves
+    of single-CTA transforms), first, middle and last vectors checked."""
+    rng = np.random.default_rng(77)
+    for log_n, batch, inverse, coset in ((10, 1500, 0, 0), (8, 3000, 1, 0), (6, 5000, 0, 1)):
+        n = 1 << log_n
+        data = rand_fr_bytes(rng, n * batch)
+        t = dev(data)
+        assert gpu_pkg.lib().zg_ntt(t.data_ptr(), log_n, batch, inverse, coset, None) == 0
+        got = host(t)
+        for b in (0, 1, batch // 2, batch - 1):
+            vec = data[b * n * 32:(b + 1) * n * 32]
+            exp = oracle.ntt(vec, inverse=bool(inverse), coset_idx=coset, coset_len=n)
+            assert got[b * n * 32:(b + 1) * n * 32] == exp, (log_n, b)
+
+
 def _neg_mont_point(p: bytes) -> bytes:
     y = int.from_bytes(p[32:], "little")
     return p[:32] + ((Q_MOD - y) % Q_MOD).to_bytes(32, "little")
