@@ -122,16 +122,19 @@ int zg_ctx_param_points(zg_ctx* ctx, int coset, int line, size_t first, size_t c
  *                    chunk); at most msm_wide_avail;
  *   ntt_cols_per_cta columns per CTA of the RS column pass: 1, 2 (default), 4;
  *   ntt_threads      threads per CTA of the three RS passes: 128, 256 (default), 512.
- * zg_ctx_autotune encodes a synthetic full-size blob on the context, times
- * each MSM product kind on a sample of the blob's MSM items (msm_ms), each
- * task size with the fastest kind (task_ms, sizes {32, 48, 64, 96}), the
- * whole blob MSM with 0 .. msm_wide_avail wide classes (wide_ms; -1 where
- * the context has no such class) and each NTT shape on the full RS
- * extension (ntt_ms[3 * i + j] for cols_per_cta {1, 2, 4}[i] and threads
- * {128, 256, 512}[j]), keeps the fastest of each and returns the choice with
- * the times (ms). It runs after the context's queued work and takes a few
- * seconds at production size; the request pipeline re-captures its CUDA
- * graphs for the new choice. */
+ * zg_ctx_autotune encodes a synthetic full-size blob on the context and
+ * times the whole blob MSM (digit sorts, bucket accumulation, combine) with
+ * each product kind and every wide class (msm_ms), with each task size and
+ * the chosen kind (task_ms, sizes {32, 48, 64, 96}); each of these twice in
+ * round-robin order, the faster time kept. Then the MSM with 0 ..
+ * msm_wide_avail wide classes (wide_ms; -1 where the context has no such
+ * class) and each NTT shape on the full RS extension (ntt_ms[3 * i + j] for
+ * cols_per_cta {1, 2, 4}[i] and threads {128, 256, 512}[j]). For the MSM
+ * choices the default (hybrid kind, task 64, every wide class) stays unless
+ * another is more than 1 % faster; for the NTT shape the fastest wins. It
+ * returns the choice with the times (ms), runs after the context's queued
+ * work and takes several seconds at production size; the request pipeline
+ * re-captures its CUDA graphs for the new choice. */
 #define ZG_MSM_PRODUCT_IMAD 0
 #define ZG_MSM_PRODUCT_HYBRID 1
 #define ZG_MSM_PRODUCT_FP64 2

@@ -362,17 +362,24 @@ def test_wide_class_choices_match_oracle(gpu_pkg, oracle):
 
 
 def test_autotune_then_encode(gpu_pkg, oracle):
-    """zg_ctx_autotune times every candidate, keeps the fastest, and the
-    encodes after it still give the oracle's bytes."""
+    """zg_ctx_autotune times every candidate and keeps the default (hybrid
+    kind, task 64) unless another is more than 1 % faster, else the fastest;
+    the encodes after it still give the oracle's bytes."""
     params = gpu_pkg.ZgEncoderParams.from_seed(6, 5, 23)
     op = oracle.params(6, 5, 23)
     t = params.autotune()
     assert t["msm_product"] in gpu_pkg.MSM_PRODUCTS
     assert all(x > 0 for x in t["msm_ms"]) and all(x > 0 for x in t["ntt_ms"])
     assert all(x > 0 for x in t["task_ms"])
-    k = gpu_pkg.MSM_PRODUCTS.index(t["msm_product"])
-    assert t["msm_ms"][k] == min(t["msm_ms"])
-    assert t["task_ms"][gpu_pkg.MSM_TASK_SIZES.index(t["msm_task"])] == min(t["task_ms"])
+
+    def picked(times, chosen, default):
+        fastest = min(range(len(times)), key=times.__getitem__)
+        if times[fastest] < 0.99 * times[default]:
+            return chosen == fastest
+        return chosen == default
+
+    assert picked(t["msm_ms"], gpu_pkg.MSM_PRODUCTS.index(t["msm_product"]), gpu_pkg.MSM_PRODUCTS.index("hybrid"))
+    assert picked(t["task_ms"], gpu_pkg.MSM_TASK_SIZES.index(t["msm_task"]), gpu_pkg.MSM_TASK_SIZES.index(64))
     assert params.tuning()["msm_product"] == t["msm_product"]
     assert params.tuning()["msm_task"] == t["msm_task"]
     payload = np.random.default_rng(5).integers(0, 256, size=4321, dtype=np.uint8).tobytes()
