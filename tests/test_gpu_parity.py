@@ -423,6 +423,33 @@ def test_device_encode_then_host_encode_are_ordered(gpu_pkg, oracle):
     params.close()
 
 
+@pytest.mark.parametrize("offset", [0, 1, 3, 8, 16])
+def test_device_encode_unaligned_payload(gpu_pkg, oracle, offset):
+    """zg_encode_device reads the caller's payload in place: at 16-byte
+    aligned addresses as 16-byte words, elsewhere byte by byte, with the
+    payload end, zero padding and length trailer byte by byte in both cases.
+    Every offset gives the oracle's encoded data, slices and roots."""
+    params = gpu_pkg.ZgEncoderParams.from_seed(4, 6, 19)
+    op = oracle.params(4, 6, 19)
+    L = gpu_pkg.lib()
+    d = params.dims
+    rng = np.random.default_rng(offset)
+    for size in (d.max_raw_data_size, 5003, 1984 * 3 + 17):
+        payload = rng.integers(0, 256, size=size, dtype=np.uint8).tobytes()
+        buf = dev(bytes(offset) + payload + bytes(32))
+        db = gpu_pkg._DeviceBlob()
+        assert L.zg_encode_device(params.handle, ctypes.c_void_p(buf.data_ptr() + offset), size, None,
+                                  ctypes.byref(db)) == 0, L.zg_last_error()
+        ob = oracle.encode(op, payload)
+        n_enc = 3 * d.raw_blob_size * 32
+        assert host(device_view(db.encoded_data, n_enc)) == ob.data(), (offset, size)
+        slices = host(device_view(db.slices, 3 * 16 * db.slice_size))
+        for i in (0, 17, 47):
+            assert slices[i * db.slice_size:(i + 1) * db.slice_size] == ob.slice(i), (offset, size, i)
+        assert host(device_view(db.file_root, 32)) == ob.file_root(), (offset, size)
+    params.close()
+
+
 @pytest.mark.parametrize("log_row", [5, 6])
 def test_encode_wide_windows_match_oracle(gpu_pkg, oracle, log_row):
     """With 1024 columns every AMT line whose nodes hold more than 1024 points
