@@ -68,7 +68,7 @@ class _DeviceBlob(ctypes.Structure):
 # ZG_MSM_PRODUCT_IMAD / _HYBRID / _FP64 / _W28 / _W28_HYBRID
 MSM_PRODUCTS = ("imad", "hybrid", "fp64", "w28", "w28_hybrid")
 MSM_TASK_SIZES = (32, 48, 64, 96)
-MSM_WIDE_MAX = 5
+MSM_WIDE_MAX = 6
 
 
 class _Tuning(ctypes.Structure):

@@ -292,10 +292,13 @@ struct zg_ctx {
   // Wide-window classes (k_wd_sort): class k sorts units of 2^ulog points
   // into 2^ulog buckets of (ulog + 1)-bit digits, for AMT lines l0 .. l0 +
   // nl - 1 (the last one the high line L - 1 when hi_last); tab[c][wl][W][N]
-  // holds their window multiples (each lane holds the sort output). The
-  // 11-bit chunk items cover the other lines, n_l0 .. n_l0 + n_lines - 1.
+  // holds their window multiples (each lane holds the sort output). With
+  // mlog = 1 its items merge pairs of sort units (units of 2^(ulog + 1)
+  // points sharing 2^ulog buckets), and the class reads the sort output of
+  // class sort_of (the first class of the same ulog, which runs the sort).
+  // The 11-bit chunk items cover the other lines, n_l0 .. n_l0 + n_lines - 1.
   struct WdClass {
-    int ulog = 0, W = 0, l0 = 0, nl = 0, hi_last = 0;
+    int ulog = 0, mlog = 0, sort_of = 0, W = 0, l0 = 0, nl = 0, hi_last = 0;
     G1Aff* tab = nullptr;
   };
   std::vector<WdClass> wd;
@@ -418,24 +421,33 @@ namespace {
 
 // Wide-window classes of a context with 1024 columns: quotient line l's nodes
 // hold 2^(lr + 9 - l) points and the high line's 2^(lr + 10), so a line takes
-// units of 2^min(15, log2 node) points when its nodes hold more than 1024. A
-// class per unit size, largest first; each class's tables are allocated only
-// with 8 GiB left over for the blob buffers and the request pipeline's slots,
-// and the first class that does not fit ends the list, so the chunk lines stay
-// one contiguous range n_l0 .. n_l0 + n_lines - 1 (the high line last when it
-// has no class).
+// units of 2^min(16, log2 node) points when its nodes hold more than 1024
+// (units of 2^16 points: pairs of 2^15-point sort units sharing their
+// buckets). A class per unit size, largest first; each class's tables are
+// allocated only with 8 GiB left over for the blob buffers and the request
+// pipeline's slots, and the first class that does not fit ends the list, so
+// the chunk lines stay one contiguous range n_l0 .. n_l0 + n_lines - 1 (the
+// high line last when it has no class).
+constexpr int WD_MERGED_LOG = WD_MAX_LOG + 1;  // largest unit: two sort units
 void plan_wide_classes(zg_ctx* c) {
   const int lr = c->lr;
   int next = 0;  // first quotient line without a class
   bool high = false;
-  for (int u = WD_MAX_LOG; u >= WD_MIN_LOG; --u) {
+  for (int u = WD_MERGED_LOG; u >= WD_MIN_LOG; --u) {
     zg_ctx::WdClass k;
-    k.ulog = u;
-    k.W = wd_windows(u);
+    k.ulog = std::min(u, WD_MAX_LOG);
+    k.mlog = u - k.ulog;
+    k.sort_of = (int)c->wd.size();
+    for (int j = 0; j < (int)c->wd.size(); ++j)
+      if (c->wd[j].ulog == k.ulog) {
+        k.sort_of = j;
+        break;
+      }
+    k.W = wd_windows(k.ulog);
     k.l0 = next;
     int nq = 0;
-    while (next + nq < lr && std::min(WD_MAX_LOG, lr + 9 - (next + nq)) == u) ++nq;
-    const bool hi = std::min(WD_MAX_LOG, lr + 10) == u;
+    while (next + nq < lr && std::min(WD_MERGED_LOG, lr + 9 - (next + nq)) == u) ++nq;
+    const bool hi = std::min(WD_MERGED_LOG, lr + 10) == u;
     if (!nq && !hi) continue;
     k.nl = nq + (hi ? 1 : 0);
     k.hi_last = hi ? 1 : 0;
@@ -470,8 +482,14 @@ void apply_wide_classes(zg_ctx* c, int on) {
 }
 
 // work items of one blob's MSM: every (coset, chunk or unit block, line),
-// the chunk lines first, then each wide class
-uint32_t blob_items(const zg_ctx* c) { return (uint32_t)(3 * c->R * c->L); }
+// the chunk lines first, then each wide class in use (a merged class has half
+// the items per line); blob_items_max bounds it for every choice of classes
+uint32_t blob_items_max(const zg_ctx* c) { return (uint32_t)(3 * c->R * c->L); }
+uint32_t blob_items(const zg_ctx* c) {
+  uint32_t u = (uint32_t)(3 * c->R * c->n_lines);
+  for (int j = 0; j < c->wd_on; ++j) u += (uint32_t)(3 * (c->R >> c->wd[j].mlog) * c->wd[j].nl);
+  return u;
+}
 
 // device bytes of a lane of `cap` blob slots (the request pipeline's
 // admission compares this with the free HBM)
@@ -481,9 +499,12 @@ size_t lane_bytes(const zg_ctx* c, int cap) {
   size_t per = 3 * (size_t)c->L * R * sizeof(XYZZ) + 3 * (4 * R - 2) * sizeof(XYZZ);
   if (c->fb) {
     per += 3 * R * (FB_BUCKETS + 1) * 4 + 3 * R * FB_WINDOWS * c->C * 2 +
-           2 * (size_t)blob_items(c) * FB_ACC_THREADS * sizeof(XYZZ);
-    for (const zg_ctx::WdClass& k : c->wd)
-      per += 3 * (N >> k.ulog) * (((size_t)1 << k.ulog) + 1) * 4 + 3 * (N >> k.ulog) * wd_unit_ents(k.ulog) * 4;
+           2 * (size_t)blob_items_max(c) * FB_ACC_THREADS * sizeof(XYZZ);
+    for (size_t j = 0; j < c->wd.size(); ++j) {
+      const zg_ctx::WdClass& k = c->wd[j];
+      if (k.sort_of == (int)j)
+        per += 3 * (N >> k.ulog) * (((size_t)1 << k.ulog) + 1) * 4 + 3 * (N >> k.ulog) * wd_unit_ents(k.ulog) * 4;
+    }
     b += (size_t)c->fb_ctas_max() * FB_MAX_TASKS * sizeof(XYZZ);
   } else {
     per += 3 * (size_t)c->L * R * MSM_WINDOWS * sizeof(XYZZ);
@@ -512,10 +533,11 @@ int alloc_lane(zg_ctx* c, Lane* ln, int cap) {
   if (c->fb) {
     ZG_CK(cudaMalloc(&ln->fb_offs, k * 3 * R * (FB_BUCKETS + 1) * sizeof(uint32_t)));
     ZG_CK(cudaMalloc(&ln->fb_ents, k * 3 * R * FB_WINDOWS * c->C * sizeof(uint16_t)));
-    ZG_CK(cudaMalloc(&ln->fb_T, k * blob_items(c) * FB_ACC_THREADS * sizeof(XYZZ)));
-    ZG_CK(cudaMalloc(&ln->fb_S, k * blob_items(c) * FB_ACC_THREADS * sizeof(XYZZ)));
+    ZG_CK(cudaMalloc(&ln->fb_T, k * blob_items_max(c) * FB_ACC_THREADS * sizeof(XYZZ)));
+    ZG_CK(cudaMalloc(&ln->fb_S, k * blob_items_max(c) * FB_ACC_THREADS * sizeof(XYZZ)));
     ln->wd.resize(c->wd.size());
     for (size_t j = 0; j < c->wd.size(); ++j) {
+      if (c->wd[j].sort_of != (int)j) continue;  // reads another class's sort output
       const size_t units = N >> c->wd[j].ulog;
       ZG_CK(cudaMalloc(&ln->wd[j].offs, k * 3 * units * (((size_t)1 << c->wd[j].ulog) + 1) * sizeof(uint32_t)));
       ZG_CK(cudaMalloc(&ln->wd[j].ents, k * 3 * units * wd_unit_ents(c->wd[j].ulog) * sizeof(uint32_t)));
@@ -766,7 +788,9 @@ BlobBufs ctx_bufs(zg_ctx* c) {
 uint64_t launches_per_encode(const zg_ctx* c, int nb = 1) {
   const int top = std::min(c->tree_depth, MERKLE_TOP_MAX);
   const uint64_t merkle = 1 + (uint64_t)(c->tree_depth - top) + (top > 0 ? 1 : 0);
-  const uint64_t per = 3 + merkle + 1 + (c->fb ? 1 + (uint64_t)c->wd_on : 2) + 1 + 1 + 1;
+  uint64_t sorts = 0;  // the wide classes in use that run their own digit sort
+  for (int k = 0; k < c->wd_on; ++k) sorts += c->wd[k].sort_of == k ? 1 : 0;
+  const uint64_t per = 3 + merkle + 1 + (c->fb ? 1 + sorts : 2) + 1 + 1 + 1;
   return per * (uint64_t)nb + (c->fb ? 2 : 0);
 }
 
@@ -794,17 +818,17 @@ FbAccArgs blob_fb_args(const zg_ctx* c, const Lane& ln, int b = 0) {
 // classes); the (T, S) partials of item u sit at fb_T / fb_S + 128 u
 uint32_t blob_wd_first_item(const zg_ctx* c, size_t k) {
   uint32_t u = (uint32_t)(3 * c->R * c->n_lines);
-  for (size_t j = 0; j < k; ++j) u += (uint32_t)(3 * c->R * c->wd[j].nl);
+  for (size_t j = 0; j < k; ++j) u += (uint32_t)(3 * (c->R >> c->wd[j].mlog) * c->wd[j].nl);
   return u;
 }
 
 // the sort output of wide class k for blob slot b
 uint32_t* lane_wd_offs(const zg_ctx* c, const Lane& ln, size_t k, int b) {
   const size_t units = c->N >> c->wd[k].ulog;
-  return ln.wd[k].offs + (size_t)b * 3 * units * (((size_t)1 << c->wd[k].ulog) + 1);
+  return ln.wd[c->wd[k].sort_of].offs + (size_t)b * 3 * units * (((size_t)1 << c->wd[k].ulog) + 1);
 }
 uint32_t* lane_wd_ents(const zg_ctx* c, const Lane& ln, size_t k, int b) {
-  return ln.wd[k].ents + (size_t)b * 3 * c->N * wd_windows(c->wd[k].ulog);
+  return ln.wd[c->wd[k].sort_of].ents + (size_t)b * 3 * c->N * wd_windows(c->wd[k].ulog);
 }
 
 // blob slot b's work items of wide class k: (coset, unit block, line)
@@ -817,12 +841,13 @@ FbAccArgs blob_wd_args(const zg_ctx* c, const Lane& ln, size_t k, int b = 0) {
   fa.ents32 = lane_wd_ents(c, ln, k, b);
   fa.outT = ln.fb_T + first;
   fa.outS = ln.fb_S + first;
-  fa.lr = c->lr;
+  fa.lr = c->lr - w.mlog;  // 2^lr items per (coset, line)
   fa.lc = c->lc;
   fa.lines = w.nl;
   fa.l0 = 0;
   fa.Ltot = w.nl;
   fa.ulog = w.ulog;
+  fa.mlog = w.mlog;
   fa.W = w.W;
   fa.tabN = c->N;
   return fa;
@@ -839,11 +864,12 @@ FbCombinePlan blob_fb_plan(const zg_ctx* c, int nb = 1) {
   for (int b = 0; b < nb; ++b) {
     const uint32_t base = (uint32_t)b * blob_items(c);
     p.start[per * b] = base;
-    p.m[per * b] = FbCombineMap{c->lr, c->n_lines, c->n_l0, c->L, 0, 0, part_blk * b};
+    p.m[per * b] = FbCombineMap{c->lr, c->n_lines, c->n_l0, c->L, 0, 0, 0, part_blk * b};
     for (size_t k = 0; k < (size_t)c->wd_on; ++k) {
       const zg_ctx::WdClass& w = c->wd[k];
       p.start[per * b + 1 + k] = base + blob_wd_first_item(c, k);
-      p.m[per * b + 1 + k] = FbCombineMap{c->lr, w.nl, w.l0, c->L, w.hi_last, w.ulog - 10, part_blk * b};
+      p.m[per * b + 1 + k] =
+          FbCombineMap{c->lr - w.mlog, w.nl, w.l0, c->L, w.hi_last, w.ulog - 10, w.mlog, part_blk * b};
     }
   }
   p.start[p.n] = (uint32_t)nb * blob_items(c);
@@ -856,7 +882,7 @@ FbCombinePlan single_fb_plan(int lr) {
   p.n = 1;
   p.start[0] = 0;
   p.start[1] = 1u << lr;
-  p.m[0] = FbCombineMap{lr, 1, 0, 1, 0, 0, 0};
+  p.m[0] = FbCombineMap{lr, 1, 0, 1, 0, 0, 0, 0};
   return p;
 }
 
@@ -1001,7 +1027,8 @@ int encode_launches(zg_ctx* c, const Lane& ln, const BlobBufs* b, int nb, const 
       k_fb_sort<<<dim3((unsigned)R, 3), 256, fb_sort_smem_bytes(lc), s>>>(b[i].enc, const_cast<uint32_t*>(fa.offs),
                                                                            const_cast<uint16_t*>(fa.ents), lr, lc, 1, N);
       for (size_t k = 0; k < (size_t)c->wd_on; ++k)
-        launch_wd_sort(c->wd[k].ulog, b[i].enc, lane_wd_offs(c, ln, k, i), lane_wd_ents(c, ln, k, i), lr, lc, N, s);
+        if (c->wd[k].sort_of == (int)k)
+          launch_wd_sort(c->wd[k].ulog, b[i].enc, lane_wd_offs(c, ln, k, i), lane_wd_ents(c, ln, k, i), lr, lc, N, s);
     }
   }
   }  // PHASE_PRE
@@ -2812,8 +2839,9 @@ int zg_ctx_autotune(zg_ctx* c, zg_tuning* out) {
       k_fb_sort<<<dim3((unsigned)c->R, 3), 256, fb_sort_smem_bytes(c->lc), s>>>(
           c->enc, const_cast<uint32_t*>(f0.offs), const_cast<uint16_t*>(f0.ents), c->lr, c->lc, 1, c->N);
       for (int k = 0; k < j; ++k)
-        launch_wd_sort(c->wd[k].ulog, c->enc, lane_wd_offs(c, c->lane, k, 0), lane_wd_ents(c, c->lane, k, 0), c->lr,
-                       c->lc, c->N, s);
+        if (c->wd[k].sort_of == k)
+          launch_wd_sort(c->wd[k].ulog, c->enc, lane_wd_offs(c, c->lane, k, 0), lane_wd_ents(c, c->lane, k, 0), c->lr,
+                         c->lc, c->N, s);
       launch_fb_accum(c, c->lane, kind, blob_acc_plan(c, c->lane, 1), s);
       launch_fb_combine(c->lane, blob_fb_plan(c, 1), s);
     };

@@ -770,7 +770,8 @@ struct FbAccArgs {
   XYZZ* outS = nullptr;
   int lr = 0, lc = 0, lines = 1;   // 2^lr items of each of `lines` lines per coset
   int l0 = 0, Ltot = 1;            // item line l reads table line l0 + l of Ltot per coset
-  int ulog = 10;                   // wide items: units of 2^ulog points
+  int ulog = 10;                   // wide items: sort units of 2^ulog points
+  int mlog = 0;                    // wide items: 2^mlog consecutive sort units share buckets
   int W = FB_WINDOWS;              // windows per table line (wd_windows(ulog) for wide items)
   uint64_t tabN = 0;               // points per window table (the param line length)
 };
@@ -787,10 +788,13 @@ struct FbAccArgs {
 //  3. task partial sums go to this CTA's scratch (gpart, L2-resident);
 //  4. thread i merges the partials of buckets 8i+1 .. 8i+8 and folds them
 //     into running sums S_i = sum B_k, T_i = sum (k - 8i) B_k.
-// Wide items (ents32 set) are 1024-bucket blocks of a wide sort unit of
-// 2^ulog points (k_wd_sort): item g of a coset is block g & (2^(ulog - 10) -
-// 1) of unit g >> (ulog - 10); its buckets' entries index the unit's points
-// and the W windows of the wide table.
+// Wide items (ents32 set) are 1024-bucket blocks of a wide unit of 2^(ulog +
+// mlog) points whose buckets are those of its 2^mlog sort units of 2^ulog
+// points (k_wd_sort; mlog <= 1): item g of a coset is block g & (2^(ulog -
+// 10) - 1) of unit g >> (ulog - 10); bucket k's entries are those of sort
+// unit 0 followed by those of sort unit 1, indexing the points of the
+// merged unit and the W windows of the wide table. A merged unit pays one
+// bucket reduction for twice the points.
 // One launch covers up to FB_MAX_SETS item sets (a blob's chunk items and its
 // wide classes, for up to FB_MAX_BLOBS blobs whose MSMs share the launch):
 // set k holds items start[k] .. start[k + 1] - 1, described by a[k] with
@@ -818,6 +822,7 @@ template <class M>
 __global__ void __launch_bounds__(FB_ACC_THREADS, FB_ACC_MIN_CTAS) k_fb_accum(const FbAccPlan plan, XYZZ* __restrict__ gpart_all,
                                                                 uint32_t* __restrict__ next, uint32_t task) {
   __shared__ uint32_t soffs[FB_BUCKETS + 1];
+  __shared__ uint32_t soffs2[FB_BUCKETS + 1];  // the second sort unit of a merged wide item
   __shared__ uint16_t tstart[FB_BUCKETS + 1];
   __shared__ uint16_t order[FB_MAX_TASKS];
   __shared__ uint16_t tbucket[FB_MAX_TASKS];
@@ -841,28 +846,40 @@ __global__ void __launch_bounds__(FB_ACC_THREADS, FB_ACC_MIN_CTAS) k_fb_accum(co
     const uint32_t l = u % a.lines, g = u / a.lines;
     const uint32_t coset = g / nch, b = g % nch;
     const uint32_t* offs;
+    const uint32_t* offs2 = nullptr;
     const uint16_t* ents = nullptr;
     const uint32_t* ents32 = a.ents32;
+    const uint32_t* ents32b = nullptr;
     const bool wide = ents32 != nullptr;
     const uint32_t ulog = (uint32_t)a.ulog;
     const G1Aff* tabl;
     if (wide) {
-      const int bl = a.ulog - 10;
+      const int bl = a.ulog - 10, ml = a.mlog;
       const uint32_t unit = b >> bl, blk = b & ((1u << bl) - 1);
-      const size_t cu = (size_t)coset * (nch >> bl) + unit;
+      const size_t cu = (size_t)coset * ((size_t)(nch >> bl) << ml) + ((size_t)unit << ml);  // first sort unit
       offs = a.offs + cu * ((1u << a.ulog) + 1) + (size_t)blk * FB_BUCKETS;
       ents32 += cu * wd_unit_ents(a.ulog);
-      tabl = a.tab + ((uint64_t)coset * a.Ltot + a.l0 + l) * a.W * N + ((uint64_t)unit << a.ulog);
+      if (ml) {
+        offs2 = offs + ((1u << a.ulog) + 1);
+        ents32b = ents32 + wd_unit_ents(a.ulog);
+      }
+      tabl = a.tab + ((uint64_t)coset * a.Ltot + a.l0 + l) * a.W * N + ((uint64_t)unit << (a.ulog + ml));
     } else {
       offs = a.offs + (size_t)g * (FB_BUCKETS + 1);
       ents = a.ents + (size_t)g * FB_WINDOWS * (1u << a.lc);
       tabl = a.tab + ((uint64_t)coset * a.Ltot + a.l0 + l) * FB_WINDOWS * N + ((uint64_t)b << a.lc);
     }
     __syncthreads();  // the previous item is finished with the shared arrays and gpart
-    for (int k = threadIdx.x; k <= FB_BUCKETS; k += blockDim.x) soffs[k] = offs[k];
+    for (int k = threadIdx.x; k <= FB_BUCKETS; k += blockDim.x) {
+      soffs[k] = offs[k];
+      soffs2[k] = offs2 ? offs2[k] : 0u;
+    }
     for (int k = threadIdx.x; k <= FB_TASK_MAX; k += blockDim.x) bins[k] = 0;
     __syncthreads();
-    const uint32_t nent = soffs[FB_BUCKETS] - soffs[0];
+    // entries of bucket k (0-based): its range in the first sort unit's list,
+    // then (merged items) its range in the second's
+    auto bcount = [&](int k) { return (soffs[k + 1] - soffs[k]) + (soffs2[k + 1] - soffs2[k]); };
+    const uint32_t nent = (soffs[FB_BUCKETS] - soffs[0]) + (soffs2[FB_BUCKETS] - soffs2[0]);
     const uint32_t cap = (uint32_t)(FB_MAX_TASKS - FB_BUCKETS);
     const uint32_t tsz = max(task, (nent + cap - 1) / cap);
     // tasks per bucket, exclusive scan -> tstart (bucket k = 0-based index)
@@ -873,7 +890,7 @@ __global__ void __launch_bounds__(FB_ACC_THREADS, FB_ACC_MIN_CTAS) k_fb_accum(co
       uint32_t sum = 0;
       for (int i = 0; i < 32; ++i) {
         const int k = lane * 32 + i;
-        const uint32_t c = soffs[k + 1] - soffs[k];
+        const uint32_t c = bcount(k);
         loc[i] = (c + tsz - 1) / tsz;
         sum += loc[i];
       }
@@ -895,7 +912,7 @@ __global__ void __launch_bounds__(FB_ACC_THREADS, FB_ACC_MIN_CTAS) k_fb_accum(co
     // task - size * task / tsz (task - size when tsz = task): larger tasks
     // first
     for (int k = threadIdx.x; k < FB_BUCKETS; k += blockDim.x) {
-      const uint32_t c = soffs[k + 1] - soffs[k];
+      const uint32_t c = bcount(k);
       for (uint32_t t = tstart[k]; t < tstart[k + 1]; ++t) {
         tbucket[t] = (uint16_t)k;
         const uint32_t j = t - tstart[k];
@@ -911,7 +928,7 @@ __global__ void __launch_bounds__(FB_ACC_THREADS, FB_ACC_MIN_CTAS) k_fb_accum(co
     __syncthreads();
     for (uint32_t t = threadIdx.x; t < ntasks; t += blockDim.x) {
       const uint32_t k = tbucket[t];
-      const uint32_t c = soffs[k + 1] - soffs[k];
+      const uint32_t c = bcount(k);
       const uint32_t j = t - tstart[k];
       const uint32_t sz = min(tsz, c - j * tsz);
       order[atomicAdd(&bins[task - sz * task / tsz], 1u)] = (uint16_t)t;
@@ -920,18 +937,22 @@ __global__ void __launch_bounds__(FB_ACC_THREADS, FB_ACC_MIN_CTAS) k_fb_accum(co
     for (uint32_t r = threadIdx.x; r < ntasks; r += blockDim.x) {
       const uint32_t t = order[r];
       const uint32_t k = tbucket[t];
-      const uint32_t e0 = soffs[k] + (t - tstart[k]) * tsz;
-      const uint32_t e1 = min(e0 + tsz, soffs[k + 1]);
+      // positions q0 .. q1 - 1 of the bucket's entries (first sort unit's
+      // c0, then the second's)
+      const uint32_t c0 = soffs[k + 1] - soffs[k];
+      const uint32_t q0 = (t - tstart[k]) * tsz;
+      const uint32_t q1 = min(q0 + tsz, bcount(k));
       XYZZ B = XYZZ::inf();
-      for (uint32_t e = e0; e < e1; ++e) {
+      for (uint32_t q = q0; q < q1; ++q) {
         uint32_t idx, w, neg;
         if (wide) {
-          const uint32_t v = ents32[e];
-          idx = v & ((1u << ulog) - 1);
+          const bool second = q >= c0;
+          const uint32_t v = second ? ents32b[soffs2[k] + (q - c0)] : ents32[soffs[k] + q];
+          idx = (v & ((1u << ulog) - 1)) + (second ? (1u << ulog) : 0u);
           w = (v >> ulog) & 31;
           neg = v >> 31;
         } else {
-          const uint32_t v = ents[e];
+          const uint32_t v = ents[soffs[k] + q];
           idx = v & 0x3ff;
           w = (v >> 10) & 31;
           neg = v >> 15;
@@ -963,8 +984,12 @@ __global__ void __launch_bounds__(FB_ACC_THREADS, FB_ACC_MIN_CTAS) k_fb_accum(co
 // Wide items (block blk = b & (2^bpu_log - 1) of a unit) add 1024 blk *
 // sum_k B_k: their buckets hold digits 1024 blk + k + 1 (bpu_log = 0 for
 // chunk items). part_off places a fused launch's blob in its own part block.
+// lr: log2 of the set's items per (coset, line); a wide set's items are
+// blocks of 2^bpu_log per unit, and a merged unit (mlog = 1) spans 2^(bpu_log
+// + mlog) part slots (one per 1024 points): its items fill the first 2^bpu_log
+// and the identity the rest, so the AMT trees sum every line's R slots alike.
 struct FbCombineMap {
-  int lr, lines, l0, L, hi_last, bpu_log;
+  int lr, lines, l0, L, hi_last, bpu_log, mlog;
   uint64_t part_off;
 };
 struct FbCombinePlan {
@@ -985,7 +1010,14 @@ __device__ __forceinline__ size_t fb_part_index(const FbCombineMap& m, uint32_t 
   const uint32_t l = v % m.lines, g = v / m.lines;
   const uint32_t nch = 1u << m.lr;
   const uint32_t line = (m.hi_last && l == (uint32_t)m.lines - 1) ? (uint32_t)m.L - 1 : (uint32_t)m.l0 + l;
-  return ((size_t)(g / nch) * m.L + line) * nch + (g % nch);
+  const uint32_t b = g % nch, bmask = (1u << m.bpu_log) - 1;
+  const uint32_t slot = ((b >> m.bpu_log) << (m.bpu_log + m.mlog)) | (b & bmask);
+  return ((size_t)(g / nch) * m.L + line) * ((size_t)nch << m.mlog) + slot;
+}
+
+// the identity in the part slots of a merged unit that no item fills
+__device__ __forceinline__ void fb_fill_unused_slots(const FbCombineMap& m, XYZZ* slot0) {
+  for (uint32_t t = 1; t < (1u << m.mlog); ++t) store_xyzz(slot0 + ((size_t)t << m.bpu_log), XYZZ::inf());
 }
 
 __device__ __forceinline__ uint32_t fb_item_block(const FbCombineMap& m, uint32_t v) {
@@ -1029,7 +1061,9 @@ __global__ void __launch_bounds__(64) k_fb_combine(const XYZZ* __restrict__ T, c
     run.add(load_xyzz(s));  // sum of all the item's buckets
     tot.add(fb_block_term(run, blk));
   }
-  store_xyzz(part + m.part_off + fb_part_index(m, v), tot);
+  XYZZ* dst = part + m.part_off + fb_part_index(m, v);
+  store_xyzz(dst, tot);
+  fb_fill_unused_slots(m, dst);
 }
 
 __device__ __forceinline__ XYZZ shfl_xor_xyzz(const XYZZ& p, int m) {
@@ -1091,7 +1125,9 @@ __global__ void __launch_bounds__(128) k_fb_combine_warp(const XYZZ* __restrict_
     tl.add(a);
     const uint32_t blk = fb_item_block(m, v);
     if (blk) tl.add(fb_block_term(U, blk));  // U at lane 0 = sum of all the item's buckets
-    store_xyzz(part + m.part_off + fb_part_index(m, v), tl);
+    XYZZ* dst = part + m.part_off + fb_part_index(m, v);
+    store_xyzz(dst, tl);
+    fb_fill_unused_slots(m, dst);
   }
 }
 

@@ -74,31 +74,51 @@ CONFIG = {
 }
 
 
-def executed_mixed_adds(lr, lc, wide_classes=5):
+def _line_unit_logs(lr, lc):
+    """Per AMT line (quotients 0 .. lr - 1, the basis, the high line): the
+    log2 of its node size and of its wide unit, min(16, log2 node) (units of
+    2^16 points are pairs of 2^15-point sort units sharing 2^15 buckets)."""
+    n = 1 << (lr + lc)
+    out = []
+    for line in range(lr + 2):
+        node = n if line == lr + 1 else (1 << lc if line == lr else n >> (line + 1))
+        lg = node.bit_length() - 1
+        out.append((lg, min(16, lg)))
+    return out
+
+
+def _wide(lc, lg, u, wide_classes):
+    # classes by unit size, largest first: class index 16 - u
+    return lc == 10 and lg > 10 and 16 - u < wide_classes
+
+
+def executed_mixed_adds(lr, lc, wide_classes=6):
     """Bucket additions of table points this build runs per blob (random
     scalars): the lines whose nodes are single chunks use 24 windows per
     point; with 1024 columns every other line uses units of 2^u points, u =
-    min(15, log2 node), and floor(254 / c) + 1 windows of c = u + 1 bits, when
-    its class (index 15 - u, largest unit first) is among the first
+    min(16, log2 node), and floor(254 / c) + 1 windows of c = min(u, 15) + 1
+    bits, when its class (index 16 - u, largest unit first) is among the first
     `wide_classes` in use, else 11-bit windows per chunk."""
     n, total = 1 << (lr + lc), 0
-    for line in range(lr + 2):
-        node = n if line == lr + 1 else (1 << lc if line == lr else n >> (line + 1))
-        u = min(15, node.bit_length() - 1)
-        if lc == 10 and node > 1024 and 15 - u < wide_classes:
-            total += 3 * n * (254 // (u + 1) + 1)
+    for lg, u in _line_unit_logs(lr, lc):
+        if _wide(lc, lg, u, wide_classes):
+            total += 3 * n * (254 // (min(u, 15) + 1) + 1)
         else:
             total += 3 * n * 24
     return total
 
 
-def executed_full_adds(lr, lc):
+def executed_full_adds(lr, lc, wide_classes=6):
     """XYZZ + XYZZ additions of the bucket reductions per blob: per MSM work
-    item (3 x lines x rows of them, 1024 buckets each) the running sums of
-    its 128 threads (two per bucket; the merges of a bucket's extra task
-    partials are not counted) and the combine of the 128 (T, S) partials
-    (2 x 127 additions plus 3 doublings)."""
-    items = 3 * (lr + 2) * (1 << lr)
+    item (1024 buckets each: 3 x rows per line, half as many on the lines of
+    2^16-point units) the running sums of its 128 threads (two per bucket;
+    the merges of a bucket's extra task partials are not counted) and the
+    combine of the 128 (T, S) partials (2 x 127 additions plus 3
+    doublings)."""
+    items = 0
+    for lg, u in _line_unit_logs(lr, lc):
+        merged = _wide(lc, lg, u, wide_classes) and u == 16
+        items += 3 * ((1 << lr) >> (1 if merged else 0))
     return items * (2 * 1024 + 2 * 127 + 3)
 
 
@@ -177,7 +197,7 @@ def parse():
                     help="which microbenchmarks --micro runs (comma-separated subset of msm,ntt,merkle; without "
                          "msm no encoder context or params are built: profiling captures of the NTT kernels)")
     ap.add_argument("--tuning", default="",
-                    help="PRODUCT,COLS,THREADS[,TASK[,WIDE_CLASSES]] (e.g. hybrid,1,256,64,5): use these kernel "
+                    help="PRODUCT,COLS,THREADS[,TASK[,WIDE_CLASSES]] (e.g. hybrid,1,256,64,6): use these kernel "
                          "choices instead of autotuning "
                          "(profiling runs, where the autotuner's own timings would be distorted)")
     ap.add_argument("--msm-window-bits", type=int, default=0,
@@ -817,9 +837,9 @@ def main():
     hbm, hbm_tag = measured_peaks()
     t_msm = phases["msm"] / 1000.0
     achieved = MSM_IMAD / t_msm / 1e9
-    wide_on = tuning.get("msm_wide_classes", 5)
+    wide_on = tuning.get("msm_wide_classes", 6)
     ex_mixed = executed_mixed_adds(LOG_ROW, LOG_COL, wide_on)
-    ex_full = executed_full_adds(LOG_ROW, LOG_COL)
+    ex_full = executed_full_adds(LOG_ROW, LOG_COL, wide_on)
     ex_prod = ex_mixed * 10 + ex_full * 14
     ex_imad = ex_prod * 264
     prod_by_kind = {k: pkg.probe_products(local, k) for k in pkg.MSM_PRODUCTS}

@@ -117,9 +117,11 @@ int zg_ctx_param_points(zg_ctx* ctx, int coset, int line, size_t first, size_t c
  *   msm_wide_classes MSM window width per AMT line: how many of the context's
  *                    wide-window classes are in use, largest unit first (class
  *                    u gives the lines whose nodes hold >= 2^u points units of
- *                    2^u points and (u + 1)-bit windows; the lines of the
- *                    classes not in use run 11-bit windows per 1024-point
- *                    chunk); at most msm_wide_avail;
+ *                    2^u points: (u + 1)-bit windows for u <= 15; u = 16 uses
+ *                    16-bit windows, pairs of 2^15-point sort units sharing
+ *                    their buckets; the lines of the classes not in use run
+ *                    11-bit windows per 1024-point chunk); at most
+ *                    msm_wide_avail;
  *   ntt_cols_per_cta columns per CTA of the RS column pass: 1, 2 (default), 4;
  *   ntt_threads      threads per CTA of the three RS passes: 128, 256 (default), 512.
  * zg_ctx_autotune encodes a synthetic full-size blob on the context and
@@ -142,7 +144,7 @@ int zg_ctx_param_points(zg_ctx* ctx, int coset, int line, size_t first, size_t c
 #define ZG_MSM_PRODUCT_W28_HYBRID 4
 #define ZG_MSM_PRODUCTS 5
 #define ZG_MSM_TASK_SIZES 4
-#define ZG_MSM_WIDE_MAX 5
+#define ZG_MSM_WIDE_MAX 6
 typedef struct zg_tuning {
   uint32_t msm_product;
   uint32_t msm_task;

@@ -339,14 +339,17 @@ def test_tuning_choices_match_oracle(gpu_pkg, oracle, product, cpb, threads, tas
     params.close()
 
 
-def test_wide_class_choices_match_oracle(gpu_pkg, oracle):
-    """At 32 x 1024 the context holds five wide-window classes; every number of
-    them in use (the lines of the others on 11-bit chunk windows) gives the
-    oracle's bytes."""
-    params = gpu_pkg.ZgEncoderParams.from_seed(5, 10, 13)
-    op = oracle.params(5, 10, 13)
+@pytest.mark.parametrize("log_row", [5, 6])
+def test_wide_class_choices_match_oracle(gpu_pkg, oracle, log_row):
+    """At 32 x 1024 the context holds five wide-window classes (units of 2^15
+    .. 2^11 points); at 64 x 1024 six, the first for the high line's 2^16-point
+    nodes as pairs of 2^15-point sort units (the 2^15 class then reads that
+    class's sort). Every number of them in use (the lines of the others on
+    11-bit chunk windows) gives the oracle's bytes."""
+    params = gpu_pkg.ZgEncoderParams.from_seed(log_row, 10, 13)
+    op = oracle.params(log_row, 10, 13)
     avail = params.tuning()["msm_wide_avail"]
-    assert avail == 5
+    assert avail == log_row
     payload = np.random.default_rng(13).integers(0, 256, size=params.dims.max_raw_data_size // 3,
                                                  dtype=np.uint8).tobytes()
     exp = oracle.encode(op, payload)
@@ -357,7 +360,7 @@ def test_wide_class_choices_match_oracle(gpu_pkg, oracle):
         r = gpu_pkg.EncoderService(params).process_data(payload, False)
         assert r.erasure_commitment == exp.commitment(), k
         assert r.encoded_slice == [exp.slice(i) for i in range(params.dims.rows_encoded)], k
-    assert lines == sorted(lines) and lines[0] == 0 and lines[-1] == 5
+    assert lines == sorted(lines) and lines[0] == 0 and lines[-1] == log_row
     params.close()
 
 
