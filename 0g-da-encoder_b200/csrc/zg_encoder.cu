@@ -925,21 +925,37 @@ FbAccPlan single_acc_plan(const FbAccArgs& fa, uint32_t units) {
   return p;
 }
 
-// the MSM items of nb blobs on a lane in one plan (the order of blob_fb_plan)
+// The MSM items of nb blobs on a lane in one plan. The sets run in order of
+// decreasing entries per item (the wide items of 2^16-point units, the chunk
+// items, then the other wide classes from 2^11-point units, 22 windows, to
+// 2^15, 16 windows), blob by blob within a kind, so that the persistent
+// kernel ends on its shortest items; each set's results still go to its
+// place in the combine's item order (blob_fb_plan).
 FbAccPlan blob_acc_plan(const zg_ctx* c, const Lane& ln, int nb = 1) {
+  struct Kind {
+    int k;  // wide class, or -1 for the chunk items
+    uint32_t ents;  // entries per item (windows x 1024 points)
+  };
+  std::vector<Kind> kinds{{-1, (uint32_t)FB_WINDOWS * 1024u}};
+  for (int k = 0; k < c->wd_on; ++k)
+    kinds.push_back({k, ((uint32_t)wd_windows(c->wd[k].ulog) * 1024u) << c->wd[k].mlog});
+  std::stable_sort(kinds.begin(), kinds.end(), [](const Kind& x, const Kind& y) { return x.ents > y.ents; });
   FbAccPlan p;
-  const int per = 1 + c->wd_on;
-  p.n = per * nb;
-  for (int b = 0; b < nb; ++b) {
-    const uint32_t base = (uint32_t)b * blob_items(c);
-    p.start[per * b] = base;
-    p.a[per * b] = blob_fb_args(c, ln, b);
-    for (size_t k = 0; k < (size_t)c->wd_on; ++k) {
-      p.start[per * b + 1 + k] = base + blob_wd_first_item(c, k);
-      p.a[per * b + 1 + k] = blob_wd_args(c, ln, k, b);
+  uint32_t at = 0;
+  for (const Kind& kd : kinds)
+    for (int b = 0; b < nb; ++b) {
+      p.start[p.n] = at;
+      if (kd.k < 0) {
+        p.a[p.n] = blob_fb_args(c, ln, b);
+        at += (uint32_t)(3 * c->R * c->n_lines);
+      } else {
+        const zg_ctx::WdClass& w = c->wd[kd.k];
+        p.a[p.n] = blob_wd_args(c, ln, (size_t)kd.k, b);
+        at += (uint32_t)(3 * (c->R >> w.mlog) * w.nl);
+      }
+      ++p.n;
     }
-  }
-  p.start[p.n] = (uint32_t)nb * blob_items(c);
+  p.start[p.n] = at;
   return p;
 }
 
